@@ -1,0 +1,259 @@
+/*
+ * speckle_b200.h -- C ABI of the B200 (sm_100a) speckle-tracking library.
+ *
+ * The library re-implements the hot path of GrIMP's speckleSource:
+ *   strack  (Strack/speckleTrack.c)  -> sb_strack()
+ *   strackw (Strackw/corrTrackFast.c) -> sb_strackw()
+ *   cullst  (Cullst/cull*.c)          -> sb_cull() and the four per-pass calls
+ * Every entry point takes plain pointers, sizes and structs of plain values.
+ * Nothing here depends on PyTorch or on any C++ type.
+ *
+ * Conventions
+ *   - Return value: SB_OK (0) or a negative SB_ERR_* code.  The library never
+ *     exits the process; sb_last_error() gives a one-line reason.
+ *   - Grids are row-major nA rows (azimuth) x nR columns (range).
+ *   - Per-point failures stay in-band exactly as in the reference:
+ *     offsets = -SB_LARGEINT (-2e9), corr = 0 or the last correlation tried,
+ *     type = SB_BAD (0).
+ *   - A context is bound to one CUDA device and is not thread-safe; use one
+ *     context per host thread.  Work is issued on the context's own stream.
+ */
+#ifndef SPECKLE_B200_H
+#define SPECKLE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SB_ABI_VERSION 1
+
+/* Status codes. */
+#define SB_OK 0
+#define SB_ERR_ARG (-1)         /* invalid argument or parameter combination */
+#define SB_ERR_CUDA (-2)        /* a CUDA call failed */
+#define SB_ERR_NOMEM (-3)       /* device or host allocation failed */
+#define SB_ERR_UNSUPPORTED (-4) /* option the reference has but this build does not */
+#define SB_ERR_NODEVICE (-5)    /* no CUDA device / kernels not loadable */
+#define SB_ERR_TIMEOUT (-6)     /* a bounded device-side wait gave up */
+
+/* Sentinel used by every output file of the reference (clib LARGEINT). */
+#define SB_LARGEINT 2000000000
+
+/* Match types written to the .mt files (Strack/speckleTrack.c:19-22). */
+#define SB_BAD 0
+#define SB_CMATCH 1
+#define SB_AMPMATCH 2
+#define SB_AMPMATCHLARGE 3
+
+/* Byte orders (Strack/strack.h:9-10). */
+#define SB_LSB 0
+#define SB_MSB 1
+
+/* Sample types of the SLC images. */
+#define SB_CFLOAT32 0 /* complex float32 (default; "floatFlag == TRUE") */
+#define SB_CINT16 1   /* complex int16 ("-integerComplex") */
+
+typedef struct sb_context sb_context;
+
+/* ------------------------------------------------------------------------ */
+/* Context                                                                   */
+/* ------------------------------------------------------------------------ */
+
+/* Create a context on CUDA device `device`.  No reference counterpart: the
+ * reference keeps its state in module globals (Strack/speckleTrack.c:89-134). */
+int sb_context_create(int device, sb_context **out);
+void sb_context_destroy(sb_context *ctx);
+/* Last error message of this context (never NULL). */
+const char *sb_last_error(const sb_context *ctx);
+/* ABI version compiled into the library. */
+int sb_abi_version(void);
+/* Device-side time (ms) of the last sb_strack/sb_strackw/sb_cull call, measured
+ * with CUDA events on the context stream, split into: [0] whole call,
+ * [1] host->device copies, [2] kernels, [3] device->host copies. */
+int sb_last_timing(const sb_context *ctx, float ms[4]);
+/* Number of kernels launched by the last call. */
+int64_t sb_last_launch_count(const sb_context *ctx);
+/* Device time (ms, CUDA events on the context stream) of the main kernels of
+ * the last sb_strack call: [0] complex stage, [1] small amplitude try,
+ * [2] large amplitude try, [3] Gaussian fits, [4] bookkeeping (select, fill,
+ * finalize); and the number of points each of [0..2] processed in [5..7]. */
+int sb_last_stage_timing(const sb_context *ctx, float ms[8]);
+
+/* ------------------------------------------------------------------------ */
+/* Inputs                                                                    */
+/* ------------------------------------------------------------------------ */
+
+/* One SLC image: na rows (azimuth) of nr complex samples (range).  The bytes
+ * are those of the image file (raw, as read by loadBuffer,
+ * Strack/speckleTrack.c:1369-1399); byteOrder says whether they must be
+ * swapped (MSB = big-endian file, the reference default). */
+typedef struct {
+    const void *data;
+    int32_t nr;
+    int32_t na;
+    int32_t sampleType; /* SB_CFLOAT32 or SB_CINT16 */
+    int32_t byteOrder;  /* SB_LSB: native little-endian; SB_MSB: swap */
+    int32_t onDevice;   /* 0: host pointer; 1: device pointer (already resident) */
+} sb_image;
+
+/* Prior offset grid used for the initial shift when polyShift == 0
+ * (Offsets read by readBothOffsetsStrack, Strack/readBothOffsetsStrack.c:79-120).
+ * Values are native floats; <= -0.9*LARGEINT means "no value". */
+typedef struct {
+    int32_t nr;
+    int32_t na;
+    double r0;
+    double a0;
+    double deltaR;
+    double deltaA;
+    const float *dr; /* na x nr, host */
+    const float *da; /* na x nr, host */
+} sb_offset_grid;
+
+/* Byte mask gating each grid point (maskData, Strack/strack.h:42-51). */
+typedef struct {
+    int32_t r0;
+    int32_t a0;
+    int32_t nr;
+    int32_t na;
+    int32_t nrl; /* range looks (sample spacing of the mask) */
+    int32_t nal; /* azimuth looks */
+    const uint8_t *mask; /* na x nr, host; values are read as signed char */
+} sb_mask;
+
+/* Baseline phase flattening (phaseCorrectBaseline, speckleTrack.c:868-907).
+ * All-zero baseline terms make the correction an exact identity, which is
+ * also what the reference computes when no baseparams file is given (the
+ * fields are then pinned to zero). */
+typedef struct {
+    double Bn, Bp, dBn, dBp, dBnQ, dBpQ;
+    double lambda;
+    /* Per range sample of image 1 (length nSlpR): sin/cos of the look-angle
+     * offset and 1/range, as tabulated by initPhaseCorrect
+     * (speckleTrack.c:1556-1625).  May be NULL when all terms are zero. */
+    const double *sinThetaD;
+    const double *cosThetaD;
+    const double *overRange;
+} sb_baseline;
+
+/* Parameters shared by strack and strackw (TrackParams, Strack/strack.h:56-165). */
+typedef struct {
+    int32_t rStart, aStart; /* first estimate (already divided by scaleFactor) */
+    int32_t deltaR, deltaA; /* grid step */
+    int32_t nR, nA;         /* grid size */
+    int32_t wR, wA;         /* complex window */
+    int32_t wRa, wAa;       /* amplitude window (strackw: search window) */
+    int32_t scaleFactor;    /* output offsets are multiplied by this */
+    /* strack flags (Strack/strack.c:137-178) */
+    int32_t noComplex;      /* -noComplex */
+    int32_t hanningFlag;    /* 1 unless -noHanning */
+    int32_t maxTries;       /* 2, or 1 with -singleAmp */
+    int32_t checkAzFocus;   /* -checkAzFocus */
+    int32_t gaussFlag;      /* -gauss: experimental 2-D fit, not supported */
+    float azDefocusThresh;  /* 1.8 in the reference CLI */
+    /* strackw parameters (parseTrack.c:222-253) */
+    int32_t edgePadR, edgePadA; /* search radius, before the internal +NFAST/4 */
+    int32_t navgR, navgA;       /* box pre-smoothing half widths (>1 enables) */
+    /* initial shift (parseInitialOffsets.c, findImage2Pos) */
+    int32_t polyShift;          /* 1: polynomial; 0: initOffsets grid */
+    double rShiftPoly[3];       /* Rshift = p0 + p1*range + p2*azimuth */
+    double aShiftPoly[3];
+    const sb_offset_grid *initOffsets; /* required when polyShift == 0 */
+    const sb_mask *mask;               /* NULL: every point is tried */
+    const sb_baseline *baseline;       /* NULL: zero baseline */
+} sb_track_params;
+
+/* ------------------------------------------------------------------------ */
+/* Outputs                                                                   */
+/* ------------------------------------------------------------------------ */
+
+/* Grids written row by row to <outputfile>.{dr,da,cc,azd,mt} by writeOffsets
+ * (Strack/sTrackOut.c:44-60).  Pointers are host memory unless onDevice. */
+typedef struct {
+    float *offR;
+    float *offA;
+    float *corr;
+    float *azd;     /* strack only; may be NULL for strackw */
+    uint8_t *type;
+    int32_t onDevice;
+    /* statistics printed by printLineSummary (speckleTrack.c:1426-1447) */
+    int64_t nComplex, nAmp, nAmpL, nFail, nAttempted;
+} sb_track_result;
+
+/* ------------------------------------------------------------------------ */
+/* Tracking                                                                  */
+/* ------------------------------------------------------------------------ */
+
+/* Replaces void speckleTrack(TrackParams *) (Strack/strack.h:170,
+ * body Strack/speckleTrack.c:159-346): complex match first, then the small
+ * and large amplitude tries, for every point of the nA x nR grid. */
+int sb_strack(sb_context *ctx, const sb_track_params *p, const sb_image *img1,
+              const sb_image *img2, sb_track_result *out);
+
+/* Replaces void corrTrackFast(TrackParams *) (Strackw/strackt.h:31,
+ * body Strackw/corrTrackFast.c:89-231): normalised amplitude correlation of a
+ * chip of image 2 inside a search window of image 1. */
+int sb_strackw(sb_context *ctx, const sb_track_params *p, const sb_image *img1,
+               const sb_image *img2, sb_track_result *out);
+
+/* Batched Doppler-carrier estimate: replaces estDopCarrier1 (Strack/strack.h:180,
+ * Strack/dopplerEstimation.c:25-40) for nPatch pairs of nAz x nRg complex
+ * patches stored contiguously (interleaved re,im float32, device pointers).
+ * azShift[k] receives the roll rescaled to wA. */
+int sb_est_dop_carrier(sb_context *ctx, const float *patches1, const float *patches2,
+                       int32_t nPatch, int32_t nAz, int32_t nRg, int32_t wA,
+                       int32_t *azShift);
+
+/* ------------------------------------------------------------------------ */
+/* Culling                                                                   */
+/* ------------------------------------------------------------------------ */
+
+/* CullParams (Cullst/cullst.h:4-59) restricted to the values the passes read. */
+typedef struct {
+    int32_t nR, nA;
+    int32_t bR, bA;        /* -boxSize (cullSTData); cullStats always uses 9 */
+    int32_t nGood;         /* -nGood */
+    float maxA, maxR;      /* -maxA -maxR */
+    int32_t sR, sA;        /* -sr -sa */
+    int32_t islandThresh;  /* -islandThresh (<=0: no island pass) */
+    float corrThresh;      /* -corrThresh */
+    int32_t singleMT;      /* -singleMT (only honoured with a mask, as in the reference) */
+    int32_t useSim;        /* -useSim */
+    int32_t connectivity;  /* island labelling: 8 (default) or 4 */
+    int32_t nCullPasses;   /* cullSTData repetitions; cullst runs 3 */
+} sb_cull_params;
+
+/* Buffers of one cull job (host memory unless onDevice).  offR/offA/type are
+ * modified in place like the reference's CullParams arrays. */
+typedef struct {
+    float *offR, *offA;   /* in/out (cullSTData edits them in place) */
+    const float *corr;    /* in */
+    uint8_t *type;        /* in/out */
+    const uint8_t *mask;  /* offsets.mask (NULL: maskFlag FALSE) */
+    const float *simR, *simA; /* -useSim offsets (NULL unless useSim) */
+    float *offRS, *offAS; /* out: smoothed offsets (.dr/.da of outbase) */
+    float *sigmaR, *sigmaA; /* out: sigmas (.sr/.sa next to inbase) */
+    int32_t onDevice;
+    int64_t nCulled;      /* out: points culled by the last cullSTData pass */
+    int64_t nIslands, nIslandPoints; /* out */
+} sb_cull_data;
+
+/* Whole cullst pipeline of Cullst/cullst.c:71-101: sim subtract, cullSTData
+ * x nCullPasses, cullStats, sim add, cullSmooth, cullIslands. */
+int sb_cull(sb_context *ctx, const sb_cull_params *p, sb_cull_data *d);
+
+/* Single passes, same buffers.  Replace cullSTData/cullStats/cullSmooth/
+ * cullIslands(CullParams *) (Cullst/cullst.h:60-66). */
+int sb_cull_st_data(sb_context *ctx, const sb_cull_params *p, sb_cull_data *d);
+int sb_cull_stats(sb_context *ctx, const sb_cull_params *p, sb_cull_data *d);
+int sb_cull_smooth(sb_context *ctx, const sb_cull_params *p, sb_cull_data *d);
+int sb_cull_islands(sb_context *ctx, const sb_cull_params *p, sb_cull_data *d);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPECKLE_B200_H */

@@ -1,0 +1,663 @@
+// capi.cu -- the library's C ABI (include/speckle_b200.h): contexts, device
+// buffers, the host-side plan of the strack grid, and the stage sequence.
+//
+// The serial per-point loop of speckleTrack (Strack/speckleTrack.c:194-338)
+// becomes:
+//   host  : plan every grid point in raster order (findImage2Pos with its
+//           carry-over of r2/a2, maskValue, boundsCheck for the three window
+//           sizes) -- cheap scalar work that keeps the reference's sequential
+//           semantics exactly;
+//   device: complex stage over the points with a complex try, then the small
+//           and the large amplitude tries over the points whose replayed
+//           control flow reaches them, then one finalize pass.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/speckle_b200.h"
+#include "capi_internal.h"
+#include "strack_device.cuh"
+#include "strack_finalize.h"
+#include "strack_fit.h"
+#include "strack_kernels.h"
+
+using namespace sbk;
+
+// ---------------------------------------------------------------- context
+
+int sb_ctx_fail(sb_context* c, int code, const char* fmt, ...)
+{
+    if (c) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof(buf), fmt, ap);
+        va_end(ap);
+        c->err = buf;
+    }
+    return code;
+}
+
+int sb_ctx_cuda(sb_context* c, cudaError_t e, const char* what)
+{
+    if (e == cudaSuccess) return SB_OK;
+    return sb_ctx_fail(c, SB_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+void* sb_ctx_buf(sb_context* c, const char* name, size_t bytes, cudaError_t* err)
+{
+    DevBuf& b = c->bufs[name];
+    if (b.bytes < bytes) {
+        if (b.ptr) cudaFree(b.ptr);
+        b.ptr = nullptr;
+        b.bytes = 0;
+        cudaError_t e = cudaMalloc(&b.ptr, bytes > 0 ? bytes : 16);
+        if (e != cudaSuccess) {
+            *err = e;
+            return nullptr;
+        }
+        b.bytes = bytes;
+    }
+    *err = cudaSuccess;
+    return b.ptr;
+}
+
+extern "C" int sb_abi_version(void) { return SB_ABI_VERSION; }
+
+extern "C" int sb_context_create(int device, sb_context** out)
+{
+    if (!out) return SB_ERR_ARG;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) return SB_ERR_NODEVICE;
+    if (device < 0 || device >= n) return SB_ERR_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return SB_ERR_NODEVICE;
+    sb_context* c = new sb_context();
+    c->device = device;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+        delete c;
+        return SB_ERR_NODEVICE;
+    }
+    c->numSM = prop.multiProcessorCount;
+    c->smMajor = prop.major;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return SB_ERR_CUDA;
+    }
+    for (int k = 0; k < 4; ++k) cudaEventCreate(&c->ev[k]);
+    for (int k = 0; k < 16; ++k) cudaEventCreate(&c->sev[k]);
+    *out = c;
+    return SB_OK;
+}
+
+extern "C" void sb_context_destroy(sb_context* c)
+{
+    if (!c) return;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    for (auto& kv : c->bufs)
+        if (kv.second.ptr) cudaFree(kv.second.ptr);
+    for (auto& kv : c->tables)
+        if (kv.second) cudaFree(kv.second);
+    for (int k = 0; k < 4; ++k) cudaEventDestroy(c->ev[k]);
+    for (int k = 0; k < 16; ++k) cudaEventDestroy(c->sev[k]);
+    cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+extern "C" const char* sb_last_error(const sb_context* c)
+{
+    if (!c) return "null context";
+    return c->err.c_str();
+}
+
+extern "C" int sb_last_timing(const sb_context* c, float ms[4])
+{
+    if (!c || !ms) return SB_ERR_ARG;
+    for (int k = 0; k < 4; ++k) ms[k] = c->timing[k];
+    return SB_OK;
+}
+
+extern "C" int64_t sb_last_launch_count(const sb_context* c) { return c ? c->launches : 0; }
+
+extern "C" int sb_last_stage_timing(const sb_context* c, float ms[8])
+{
+    if (!c || !ms) return SB_ERR_ARG;
+    for (int k = 0; k < 8; ++k) ms[k] = c->stage[k];
+    return SB_OK;
+}
+
+// ---------------------------------------------------------------- tables
+
+// Host-computed constant tables (double precision, rounded once to float).
+const void* sb_table(sb_context* c, const std::string& key, const std::vector<float2>& host)
+{
+    auto it = c->tables.find(key);
+    if (it != c->tables.end()) return it->second;
+    void* d = nullptr;
+    if (cudaMalloc(&d, host.size() * sizeof(float2)) != cudaSuccess) return nullptr;
+    cudaMemcpy(d, host.data(), host.size() * sizeof(float2), cudaMemcpyHostToDevice);
+    c->tables[key] = d;
+    return d;
+}
+
+static const double kPi = 3.14159265358979323846;
+
+const float2* tw_table(sb_context* c, int N)
+{
+    std::vector<float2> h(N);
+    for (int e = 0; e < N; ++e) {
+        double ang = -2.0 * kPi * (double)e / (double)N;
+        h[e] = make_float2((float)cos(ang), (float)sin(ang));
+    }
+    return (const float2*)sb_table(c, "tw" + std::to_string(N), h);
+}
+
+// tau_1[k'] = +exp(+2 pi i k'/(2W)) for k' < W/2, -exp(...) for k' >= W/2.
+const float2* tau_table(sb_context* c, int W)
+{
+    std::vector<float2> h(W);
+    for (int k = 0; k < W; ++k) {
+        double ang = 2.0 * kPi * (double)k / (2.0 * W);
+        double sgn = (k < W / 2) ? 1.0 : -1.0;
+        h[k] = make_float2((float)(sgn * cos(ang)), (float)(sgn * sin(ang)));
+    }
+    return (const float2*)sb_table(c, "tau" + std::to_string(W), h);
+}
+
+// A[n][t] = sum_{f=-4..3} exp(+2 pi i f (n - 12 t)/96), n = 24..71.
+const float2* osA_table(sb_context* c)
+{
+    std::vector<float2> h(OSW * NFAST);
+    for (int n = 0; n < OSW; ++n)
+        for (int t = 0; t < NFAST; ++t) {
+            double re = 0, im = 0;
+            const int d = (n + 24) - NOVER * t;
+            for (int f = -NFAST / 2; f < NFAST / 2; ++f) {
+                double ang = 2.0 * kPi * (double)f * (double)d / (double)(NFAST * NOVER);
+                re += cos(ang);
+                im += sin(ang);
+            }
+            h[n * NFAST + t] = make_float2((float)re, (float)im);
+        }
+    return (const float2*)sb_table(c, "osA", h);
+}
+
+// computeHanning (speckleTrack.c:1830-1852), W x W, square windows.
+const float* hanning_table(sb_context* c, int W)
+{
+    std::vector<float2> h((W * W + 1) / 2);
+    float* f = reinterpret_cast<float*>(h.data());
+    for (int i = 0; i < W / 2; i++) {
+        int i1 = W / 2 + i, i2 = W / 2 - i - 1;
+        double wi = 0.5 * (1.0 + cos((2.0 * kPi) * (double)i / (double)(W - 1)));
+        for (int j = 0; j < W / 2; j++) {
+            int j1 = W / 2 + j, j2 = W / 2 - j - 1;
+            double wj = 0.5 * (1.0 + cos((2.0 * kPi) * (double)j / (double)(W - 1)));
+            float v = (float)(wi * wj);
+            f[i1 * W + j1] = v;
+            f[i2 * W + j2] = v;
+            f[i2 * W + j1] = v;
+            f[i1 * W + j2] = v;
+        }
+    }
+    return (const float*)sb_table(c, "han" + std::to_string(W), h);
+}
+
+// ---------------------------------------------------------------- planning
+
+static int inBounds(int r1, int a1, int wR, int wA, int sR, int sA)
+{
+    return (r1 > 0 && (r1 + wR) < sR && a1 > 0 && (a1 + wA) < sA);  // speckleTrack.c:1943-1946
+}
+
+// getShifts, speckleTrack.c:1857-1940.
+static void getShifts(double range, double azimuth, const sb_offset_grid* o, double* dr, double* da)
+{
+    float minvalue = (float)((float)-SB_LARGEINT * 0.9);
+    range = (range - o->r0) / o->deltaR;
+    azimuth = (azimuth - o->a0) / o->deltaA;
+    if (range < 0.0 || azimuth < 0.0 || (int)range >= o->nr || (int)azimuth >= o->na) {
+        *dr = -SB_LARGEINT;
+        *da = -SB_LARGEINT;
+        return;
+    }
+    int j = (int)range, i = (int)azimuth;
+    const int nr = o->nr;
+    const float *R = o->dr, *A = o->da;
+    if (j == (o->nr - 1) || i == (o->na - 1)) {
+        *dr = R[(size_t)i * nr + j];
+        *da = A[(size_t)i * nr + j];
+        if (*dr < minvalue || *da < minvalue) {
+            *dr = -SB_LARGEINT;
+            *da = -SB_LARGEINT;
+        }
+        return;
+    }
+    float t = (float)(range - (double)j), u = (float)(azimuth - (double)i);
+    const float* img[2] = {R, A};
+    double* outv[2] = {dr, da};
+    for (int q = 0; q < 2; ++q) {
+        const float* M = img[q];
+        float p1 = M[(size_t)i * nr + j], p2 = M[(size_t)i * nr + j + 1];
+        float p3 = M[(size_t)(i + 1) * nr + j + 1], p4 = M[(size_t)(i + 1) * nr + j];
+        if (p1 <= minvalue || p2 <= minvalue || p3 <= minvalue || p4 <= minvalue) {
+            float mx = fmaxf(fmaxf(fmaxf(p1, p2), p3), p4);
+            *outv[q] = mx;
+            if (*outv[q] < minvalue) {
+                *dr = -SB_LARGEINT;
+                *da = -SB_LARGEINT;
+                return;
+            }
+        } else {
+            *outv[q] = (float)((1.0 - t) * (1.0 - u) * p1 + t * (1.0 - u) * p2 + t * u * p3 + (1.0 - t) * u * p4);
+        }
+    }
+}
+
+// findImage2Pos, speckleTrack.c:810-847 (keeps r2/a2 when the grid has no value).
+static void findImage2Pos(const sb_track_params* p, int r1, int a1, int* r2, int* a2)
+{
+    double aShift = 0, rShift = 0, sc = (double)p->scaleFactor;
+    int haveShift = 0;
+    if (p->polyShift == 0) {
+        getShifts(r1, a1, p->initOffsets, &rShift, &aShift);
+        if (rShift > (-SB_LARGEINT + 1))
+            haveShift = 1;
+        else
+            return;
+    }
+    if (p->polyShift != 0 || haveShift == 0) {
+        rShift = p->rShiftPoly[0] + (double)(r1 * sc) * p->rShiftPoly[1] + (double)(a1 * sc) * p->rShiftPoly[2];
+        aShift = p->aShiftPoly[0] + (double)(r1 * sc) * p->aShiftPoly[1] + (double)(a1 * sc) * p->aShiftPoly[2];
+    }
+    rShift /= sc;
+    aShift /= sc;
+    *r2 = (rShift >= 0) ? r1 + (int)(rShift + 0.5) : r1 + (int)(rShift - 0.5);
+    *a2 = (aShift >= 0) ? a1 + (int)(aShift + 0.5) : a1 + (int)(aShift - 0.5);
+}
+
+// maskValue, speckleTrack.c:1951-1965.
+static int maskValue(const sb_track_params* p, int r1, int a1)
+{
+    const sb_mask* m = p->mask;
+    if (!m) return 1;
+    int ia1 = (a1 + p->wA / 2 - m->a0) / m->nal;
+    int ir1 = (r1 + p->wR / 2 - m->r0) / m->nrl;
+    if (ia1 < 0 || ia1 >= m->na || ir1 < 0 || ir1 >= m->nr) return 0;
+    return (int)(signed char)m->mask[(size_t)ia1 * m->nr + ir1];
+}
+
+static void plan_strack(const sb_track_params* p, int nr1, int na1, int nr2, int na2, std::vector<PointPlan>& plan,
+                        std::vector<int>& clist)
+{
+    const int nR = p->nR, nA = p->nA;
+    plan.resize((size_t)nR * nA);
+    clist.clear();
+    int r2 = 0, a2 = 0;  // uninitialised in the reference: pinned to 0
+    for (int i = 0; i < nA; i++) {
+        const int a1 = p->aStart + i * p->deltaA - p->wA / 2;
+        for (int j = 0; j < nR; j++) {
+            const int r1 = p->rStart + j * p->deltaR - p->wR / 2;
+            findImage2Pos(p, r1, a1, &r2, &a2);
+            int maskVal = maskValue(p, r1 * p->scaleFactor, a1 * p->scaleFactor);
+            maskVal = maskVal < 1 ? maskVal : 1;
+            PointPlan pl;
+            pl.r1 = r1;
+            pl.a1 = a1;
+            pl.r2 = r2;
+            pl.a2 = a2;
+            pl.flags = 0;
+            if (maskVal > 0) pl.flags |= PF_MASK;
+            if (inBounds(r1, a1, p->wR, p->wA, nr1, na1) && inBounds(r2, a2, p->wR, p->wA, nr2, na2))
+                pl.flags |= PF_CBOUND;
+            for (int s = 1; s <= 2; ++s) {
+                const int a1a = p->aStart + i * p->deltaA - p->wA / 2 * s;
+                const int r1a = p->rStart + j * p->deltaR - p->wR / 2 * s;
+                const int r2a = r1a + (r2 - r1), a2a = a1a + (a2 - a1);
+                if (inBounds(r1a, a1a, p->wRa * s, p->wAa * s, nr1, na1) &&
+                    inBounds(r2a, a2a, p->wRa * s, p->wAa * s, nr2, na2))
+                    pl.flags |= (s == 1 ? PF_SBOUND : PF_LBOUND);
+            }
+            const size_t k = (size_t)i * nR + j;
+            plan[k] = pl;
+            if ((pl.flags & PF_CBOUND) && (pl.flags & PF_MASK) && p->noComplex == 0) clist.push_back((int)k);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- images
+
+// Device view of an input image (uploads host images into a context buffer).
+int sb_image_to_device(sb_context* c, const sb_image* im, const char* name, const void** dptr)
+{
+    const size_t elem = im->sampleType == SB_CFLOAT32 ? 8 : 4;
+    const size_t bytes = (size_t)im->nr * (size_t)im->na * elem;
+    if (im->onDevice) {
+        *dptr = im->data;
+        return SB_OK;
+    }
+    cudaError_t e;
+    void* d = sb_ctx_buf(c, name, bytes, &e);
+    if (!d) return sb_ctx_cuda(c, e, "cudaMalloc(image)");
+    e = cudaMemcpyAsync(d, im->data, bytes, cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return sb_ctx_cuda(c, e, "cudaMemcpyAsync(image)");
+    *dptr = d;
+    return SB_OK;
+}
+
+static int check_image(sb_context* c, const sb_image* im)
+{
+    if (!im || !im->data || im->nr <= 0 || im->na <= 0) return sb_ctx_fail(c, SB_ERR_ARG, "invalid image");
+    if (im->sampleType != SB_CFLOAT32 && im->sampleType != SB_CINT16)
+        return sb_ctx_fail(c, SB_ERR_ARG, "invalid sampleType %d", im->sampleType);
+    if (im->byteOrder != SB_LSB && im->byteOrder != SB_MSB)
+        return sb_ctx_fail(c, SB_ERR_ARG, "invalid byteOrder %d", im->byteOrder);
+    return SB_OK;
+}
+
+// Copies (or aliases) an output grid.
+static int out_copy(sb_context* c, void* dst, const void* src, size_t bytes, int onDevice)
+{
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                    c->stream);
+    return sb_ctx_cuda(c, e, "cudaMemcpyAsync(output)");
+}
+
+static FitArgs make_fit_args(const sb_track_params* p, FitJob* fit, int nList, int stage, PointRec* rec)
+{
+    FitArgs f;
+    f.fit = fit;
+    f.nList = nList;
+    f.stage = stage;
+    f.wR = p->wR; f.wA = p->wA; f.wRa = p->wRa; f.wAa = p->wAa;
+    f.noComplex = p->noComplex;
+    f.azThresh = p->azDefocusThresh;
+    f.checkAzFocus = p->checkAzFocus;
+    f.rec = rec;
+    return f;
+}
+
+#define CK(call, what)                                               \
+    do {                                                             \
+        cudaError_t _e = (call);                                     \
+        if (_e != cudaSuccess) return sb_ctx_cuda(c, _e, what);      \
+    } while (0)
+
+// ---------------------------------------------------------------- strack
+
+extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image* img1, const sb_image* img2,
+                         sb_track_result* out)
+{
+    if (!c) return SB_ERR_ARG;
+    c->err.clear();
+    c->launches = 0;
+    if (!p || !out) return sb_ctx_fail(c, SB_ERR_ARG, "null params or result");
+    int rc;
+    if ((rc = check_image(c, img1)) != SB_OK || (rc = check_image(c, img2)) != SB_OK) return rc;
+    if (img1->sampleType != img2->sampleType) return sb_ctx_fail(c, SB_ERR_ARG, "images differ in sample type");
+    if (img1->byteOrder != img2->byteOrder) return sb_ctx_fail(c, SB_ERR_ARG, "images differ in byte order");
+    if (p->nR <= 0 || p->nA <= 0) return sb_ctx_fail(c, SB_ERR_ARG, "empty grid nR=%d nA=%d", p->nR, p->nA);
+    if ((int64_t)p->nR * p->nA > (int64_t)1 << 30) return sb_ctx_fail(c, SB_ERR_ARG, "grid too large");
+    if (p->scaleFactor <= 0) return sb_ctx_fail(c, SB_ERR_ARG, "scaleFactor must be positive");
+    if (p->gaussFlag) return sb_ctx_fail(c, SB_ERR_UNSUPPORTED, "-gauss (experimental 2-D fit) is not supported");
+    if (p->polyShift == 0 && !p->initOffsets) return sb_ctx_fail(c, SB_ERR_ARG, "polyShift=0 needs initOffsets");
+    if (p->mask && (p->mask->nal <= 0 || p->mask->nrl <= 0 || !p->mask->mask))
+        return sb_ctx_fail(c, SB_ERR_ARG, "invalid mask");
+    if (!out->offR || !out->offA || !out->corr || !out->type)
+        return sb_ctx_fail(c, SB_ERR_ARG, "null output grid");
+    const int W = p->wR;
+    if (p->wR != p->wA) return sb_ctx_fail(c, SB_ERR_UNSUPPORTED, "complex window must be square (wr == wa)");
+    if (p->noComplex == 0 && !cmplx_supported(W))
+        return sb_ctx_fail(c, SB_ERR_UNSUPPORTED, "complex window %d not supported", W);
+    const int WA = p->wRa;
+    if (p->maxTries > 0) {
+        if (p->wRa != p->wAa) return sb_ctx_fail(c, SB_ERR_UNSUPPORTED, "amplitude window must be square");
+        if (!amp_supported(WA)) return sb_ctx_fail(c, SB_ERR_UNSUPPORTED, "amplitude window %d not supported", WA);
+        if (p->maxTries > 1 && !amp_supported(WA * LA))
+            return sb_ctx_fail(c, SB_ERR_UNSUPPORTED, "large amplitude window %d not supported", WA * LA);
+    }
+    const sb_baseline* bl = p->baseline;
+    const int baseOn =
+        bl && (bl->Bn != 0 || bl->Bp != 0 || bl->dBn != 0 || bl->dBp != 0 || bl->dBnQ != 0 || bl->dBpQ != 0);
+    if (baseOn && (!bl->sinThetaD || !bl->cosThetaD || !bl->overRange))
+        return sb_ctx_fail(c, SB_ERR_ARG, "baseline tables missing");
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    cudaEventRecord(c->ev[0], c->stream);
+    for (int k = 0; k < 8; ++k) c->stage[k] = 0.f;
+
+    // ---- plan: host loop when the initial shift comes from an offset grid
+    // (its carry-over of r2/a2 is sequential), device kernel for a polynomial
+    const int n = p->nR * p->nA;
+    const bool devPlan = p->polyShift != 0;
+    std::vector<PointPlan> plan;
+    std::vector<int> clist;
+    if (!devPlan) plan_strack(p, img1->nr, img1->na, img2->nr, img2->na, plan, clist);
+
+    const void *d1, *d2;
+    if ((rc = sb_image_to_device(c, img1, "img1", &d1)) != SB_OK) return rc;
+    if ((rc = sb_image_to_device(c, img2, "img2", &d2)) != SB_OK) return rc;
+    cudaError_t e;
+    PointPlan* dplan = (PointPlan*)sb_ctx_buf(c, "plan", sizeof(PointPlan) * n, &e);
+    PointRec* drec = (PointRec*)sb_ctx_buf(c, "rec", sizeof(PointRec) * n, &e);
+    int* dlist = (int*)sb_ctx_buf(c, "list", sizeof(int) * (n + 1), &e);
+    FitJob* dfit = (FitJob*)sb_ctx_buf(c, "fit", sizeof(FitJob) * (n + 1), &e);
+    int* dcount = (int*)sb_ctx_buf(c, "count", sizeof(int) * 4, &e);
+    unsigned long long* dstats = (unsigned long long*)sb_ctx_buf(c, "stats", sizeof(unsigned long long) * 8, &e);
+    float* dR = (float*)sb_ctx_buf(c, "offR", sizeof(float) * n, &e);
+    float* dA = (float*)sb_ctx_buf(c, "offA", sizeof(float) * n, &e);
+    float* dC = (float*)sb_ctx_buf(c, "corr", sizeof(float) * n, &e);
+    float* dZ = (float*)sb_ctx_buf(c, "azd", sizeof(float) * n, &e);
+    uint8_t* dT = (uint8_t*)sb_ctx_buf(c, "type", n, &e);
+    if (!dplan || !drec || !dlist || !dfit || !dcount || !dstats || !dR || !dA || !dC || !dZ || !dT)
+        return sb_ctx_fail(c, SB_ERR_NOMEM, "device allocation failed");
+    int nC = 0;
+    if (devPlan) {
+        PlanArgs pa;
+        memset(&pa, 0, sizeof(pa));
+        pa.rStart = p->rStart; pa.aStart = p->aStart; pa.deltaR = p->deltaR; pa.deltaA = p->deltaA;
+        pa.nR = p->nR; pa.nA = p->nA;
+        pa.wR = p->wR; pa.wA = p->wA; pa.wRa = p->wRa; pa.wAa = p->wAa;
+        pa.scaleFactor = p->scaleFactor;
+        pa.noComplex = p->noComplex;
+        for (int k = 0; k < 3; ++k) {
+            pa.rPoly[k] = p->rShiftPoly[k];
+            pa.aPoly[k] = p->aShiftPoly[k];
+        }
+        pa.nr1 = img1->nr; pa.na1 = img1->na; pa.nr2 = img2->nr; pa.na2 = img2->na;
+        if (p->mask) {
+            const size_t mb = (size_t)p->mask->nr * p->mask->na;
+            uint8_t* dm = (uint8_t*)sb_ctx_buf(c, "mask", mb, &e);
+            if (!dm) return sb_ctx_fail(c, SB_ERR_NOMEM, "device allocation failed");
+            CK(cudaMemcpyAsync(dm, p->mask->mask, mb, cudaMemcpyHostToDevice, c->stream), "mask");
+            pa.mask = dm;
+            pa.mR0 = p->mask->r0; pa.mA0 = p->mask->a0; pa.mNr = p->mask->nr; pa.mNa = p->mask->na;
+            pa.mNrl = p->mask->nrl; pa.mNal = p->mask->nal;
+        }
+        CK(cudaMemsetAsync(dcount, 0, sizeof(int), c->stream), "memset");
+        CK(launch_plan_poly(pa, dplan, dlist, dcount, c->stream), "plan_poly");
+        c->launches++;
+        CK(cudaMemcpyAsync(&nC, dcount, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "count");
+        CK(cudaStreamSynchronize(c->stream), "sync");
+    } else {
+        CK(cudaMemcpyAsync(dplan, plan.data(), sizeof(PointPlan) * n, cudaMemcpyHostToDevice, c->stream), "plan");
+        if (!clist.empty())
+            CK(cudaMemcpyAsync(dlist, clist.data(), sizeof(int) * clist.size(), cudaMemcpyHostToDevice, c->stream),
+               "list");
+        nC = (int)clist.size();
+    }
+    const double *dSin = nullptr, *dCos = nullptr, *dOver = nullptr;
+    if (baseOn) {
+        const size_t nb = sizeof(double) * (size_t)img1->nr;
+        double* b = (double*)sb_ctx_buf(c, "baseTabs", 3 * nb, &e);
+        if (!b) return sb_ctx_fail(c, SB_ERR_NOMEM, "device allocation failed");
+        CK(cudaMemcpyAsync(b, bl->sinThetaD, nb, cudaMemcpyHostToDevice, c->stream), "baseline");
+        CK(cudaMemcpyAsync((char*)b + nb, bl->cosThetaD, nb, cudaMemcpyHostToDevice, c->stream), "baseline");
+        CK(cudaMemcpyAsync((char*)b + 2 * nb, bl->overRange, nb, cudaMemcpyHostToDevice, c->stream), "baseline");
+        dSin = b;
+        dCos = (const double*)((char*)b + nb);
+        dOver = (const double*)((char*)b + 2 * nb);
+    }
+    cudaEventRecord(c->ev[1], c->stream);
+
+    // ---- kernels
+    CK(launch_rec_init(drec, n, c->stream), "rec_init");
+    c->launches++;
+    CK(cudaMemsetAsync(dstats, 0, sizeof(unsigned long long) * 8, c->stream), "memset");
+    if (nC > 0) {
+        CmplxArgs a;
+        memset(&a, 0, sizeof(a));
+        a.img1 = d1;
+        a.img2 = d2;
+        a.nr1 = img1->nr; a.na1 = img1->na; a.nr2 = img2->nr; a.na2 = img2->na;
+        a.sampleType = img1->sampleType;
+        a.byteOrder = img1->byteOrder;
+        a.plan = dplan;
+        a.list = dlist;
+        a.nList = nC;
+        a.hanning = p->hanningFlag ? hanning_table(c, W) : nullptr;
+        a.hanCorr = p->hanningFlag ? 1.5 : 1.0;
+        a.twW = tw_table(c, W);
+        a.tau = tau_table(c, W);
+        a.osA = osA_table(c);
+        a.azThresh = p->azDefocusThresh;
+        a.checkAzFocus = p->checkAzFocus;
+        a.noComplex = p->noComplex;
+        a.baseOn = baseOn;
+        if (baseOn) {
+            a.Bn = bl->Bn; a.Bp = bl->Bp; a.dBn = bl->dBn; a.dBp = bl->dBp; a.dBnQ = bl->dBnQ; a.dBpQ = bl->dBpQ;
+            a.lambda = bl->lambda;
+            a.sinThetaD = dSin; a.cosThetaD = dCos; a.overRange = dOver;
+        }
+        a.rec = drec;
+        a.fit = dfit;
+        if (!a.twW || !a.tau || !a.osA || (p->hanningFlag && !a.hanning))
+            return sb_ctx_fail(c, SB_ERR_NOMEM, "table allocation failed");
+        int bpsm = cmplx_blocks_per_sm(W);
+        if (bpsm <= 0) return sb_ctx_fail(c, SB_ERR_CUDA, "complex kernel cannot be resident (W=%d)", W);
+        int nCta = c->numSM * bpsm;
+        if (nCta > a.nList) nCta = a.nList;
+        cudaEventRecord(c->sev[0], c->stream);
+        CK(launch_strack_cmplx(W, a, nCta, c->stream), "strack_cmplx");
+        c->launches++;
+        cudaEventRecord(c->sev[1], c->stream);
+        FitArgs f = make_fit_args(p, dfit, a.nList, 0, drec);
+        CK(launch_strack_fit(f, c->stream), "strack_fit");
+        c->launches++;
+        cudaEventRecord(c->sev[2], c->stream);
+        c->stage[5] = (float)a.nList;
+    }
+    WalkParams w;
+    w.wR = p->wR; w.wA = p->wA; w.wRa = p->wRa; w.wAa = p->wAa;
+    w.noComplex = p->noComplex;
+    w.maxTries = p->maxTries;
+    const bool ownAz = (p->wRa == p->wR && p->wAa == p->wA);
+    int* dAz = nullptr;
+    if (nC > 0) {
+        CK(cudaStreamSynchronize(c->stream), "sync");
+        float t0 = 0, t1 = 0;
+        cudaEventElapsedTime(&t0, c->sev[0], c->sev[1]);
+        cudaEventElapsedTime(&t1, c->sev[1], c->sev[2]);
+        c->stage[0] = t0;
+        c->stage[3] += t1;
+    }
+    for (int stage = 1; stage <= 2 && stage <= p->maxTries; ++stage) {
+        CK(cudaMemsetAsync(dcount, 0, sizeof(int), c->stream), "memset");
+        CK(launch_select(dplan, drec, n, w, stage, dlist, dcount, c->stream), "select");
+        c->launches++;
+        int cnt = 0;
+        CK(cudaMemcpyAsync(&cnt, dcount, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "count");
+        CK(cudaStreamSynchronize(c->stream), "sync");
+        if (cnt == 0) continue;
+        const int Ws = WA * (stage == 1 ? 1 : LA);
+        const bool needFill = !ownAz && !(p->noComplex && stage == 1);
+        if (needFill) {
+            dAz = (int*)sb_ctx_buf(c, "azEff", sizeof(int) * n, &e);
+            if (!dAz) return sb_ctx_fail(c, SB_ERR_NOMEM, "device allocation failed");
+            CK(launch_az_fill(drec, n, dAz, c->stream), "az_fill");
+            c->launches++;
+        }
+        AmpArgs a;
+        memset(&a, 0, sizeof(a));
+        a.img1 = d1;
+        a.img2 = d2;
+        a.nr1 = img1->nr; a.na1 = img1->na; a.nr2 = img2->nr; a.na2 = img2->na;
+        a.sampleType = img1->sampleType;
+        a.byteOrder = img1->byteOrder;
+        a.plan = dplan;
+        a.list = dlist;
+        a.nList = cnt;
+        a.stage = stage;
+        a.s = stage == 1 ? 1 : LA;
+        a.wR = p->wR; a.wA = p->wA; a.wRa = p->wRa; a.wAa = p->wAa;
+        a.nR = p->nR;
+        a.rStart = p->rStart; a.aStart = p->aStart; a.deltaR = p->deltaR; a.deltaA = p->deltaA;
+        a.noComplex = p->noComplex;
+        a.azThresh = p->azDefocusThresh;
+        a.checkAzFocus = p->checkAzFocus;
+        a.azEff = needFill ? dAz : nullptr;
+        a.twWs = tw_table(c, Ws);
+        a.tw2Ws = tw_table(c, 2 * Ws);
+        a.tau = tau_table(c, Ws);
+        a.osA = osA_table(c);
+        a.rec = drec;
+        a.fit = dfit;
+        int nCta = c->numSM * 2;
+        if (nCta > cnt) nCta = cnt;
+        a.scratchPerCta = amp_scratch_elems(Ws);
+        a.scratch = (float2*)sb_ctx_buf(c, "ampScratch", sizeof(float2) * a.scratchPerCta * nCta, &e);
+        if (!a.scratch || !a.twWs || !a.tw2Ws || !a.tau || !a.osA)
+            return sb_ctx_fail(c, SB_ERR_NOMEM, "amplitude workspace allocation failed");
+        cudaEventRecord(c->sev[2 + 2 * stage], c->stream);
+        CK(launch_strack_amp(Ws, a, nCta, c->stream), "strack_amp");
+        c->launches++;
+        cudaEventRecord(c->sev[3 + 2 * stage], c->stream);
+        FitArgs f = make_fit_args(p, dfit, cnt, stage, drec);
+        CK(launch_strack_fit(f, c->stream), "strack_fit");
+        c->launches++;
+        CK(cudaStreamSynchronize(c->stream), "sync");
+        float t0 = 0, t1 = 0;
+        cudaEventElapsedTime(&t0, c->sev[2 + 2 * stage], c->sev[3 + 2 * stage]);
+        c->stage[stage] = t0;
+        c->stage[5 + stage] = (float)cnt;
+        cudaEventRecord(c->sev[8 + stage], c->stream);
+        cudaEventSynchronize(c->sev[8 + stage]);
+        cudaEventElapsedTime(&t1, c->sev[3 + 2 * stage], c->sev[8 + stage]);
+        c->stage[3] += t1;
+    }
+    CK(launch_finalize(dplan, drec, n, w, p->scaleFactor, dR, dA, dC, dZ, dT, dstats, c->stream), "finalize");
+    c->launches++;
+    cudaEventRecord(c->ev[2], c->stream);
+
+    // ---- outputs
+    if ((rc = out_copy(c, out->offR, dR, sizeof(float) * n, out->onDevice)) != SB_OK) return rc;
+    if ((rc = out_copy(c, out->offA, dA, sizeof(float) * n, out->onDevice)) != SB_OK) return rc;
+    if ((rc = out_copy(c, out->corr, dC, sizeof(float) * n, out->onDevice)) != SB_OK) return rc;
+    if (out->azd && (rc = out_copy(c, out->azd, dZ, sizeof(float) * n, out->onDevice)) != SB_OK) return rc;
+    if ((rc = out_copy(c, out->type, dT, n, out->onDevice)) != SB_OK) return rc;
+    unsigned long long st[8];
+    CK(cudaMemcpyAsync(st, dstats, sizeof(st), cudaMemcpyDeviceToHost, c->stream), "stats");
+    cudaEventRecord(c->ev[3], c->stream);
+    CK(cudaStreamSynchronize(c->stream), "strack");
+    out->nComplex = (int64_t)st[0];
+    out->nAmp = (int64_t)st[1];
+    out->nAmpL = (int64_t)st[2];
+    out->nFail = (int64_t)st[3];
+    out->nAttempted = (int64_t)n - (int64_t)st[4];
+    cudaEventElapsedTime(&c->timing[0], c->ev[0], c->ev[3]);
+    cudaEventElapsedTime(&c->timing[1], c->ev[0], c->ev[1]);
+    cudaEventElapsedTime(&c->timing[2], c->ev[1], c->ev[2]);
+    cudaEventElapsedTime(&c->timing[3], c->ev[2], c->ev[3]);
+    {
+        float tk = c->timing[2] - c->stage[0] - c->stage[1] - c->stage[2] - c->stage[3];
+        c->stage[4] = tk > 0 ? tk : 0.f;
+    }
+    return SB_OK;
+}

@@ -1,0 +1,36 @@
+// capi_internal.h -- the context object behind sb_context and helpers shared
+// by the C-ABI translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <string>
+
+#include "../../include/speckle_b200.h"
+
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+
+struct sb_context {
+    int device = 0;
+    int numSM = 0;
+    int smMajor = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    float timing[4] = {0, 0, 0, 0};
+    float stage[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    cudaEvent_t sev[16] = {};  // per-stage event pairs
+    int nsev = 0;
+    int64_t launches = 0;
+    std::string err;
+    std::map<std::string, DevBuf> bufs;   // grown on demand, reused across calls
+    std::map<std::string, void*> tables;  // constant tables
+};
+
+int sb_ctx_fail(sb_context* c, int code, const char* fmt, ...);
+int sb_ctx_cuda(sb_context* c, cudaError_t e, const char* what);
+void* sb_ctx_buf(sb_context* c, const char* name, size_t bytes, cudaError_t* err);
+int sb_image_to_device(sb_context* c, const sb_image* im, const char* name, const void** dptr);
+const float2* tw_table(sb_context* c, int N);

@@ -1,0 +1,303 @@
+// fft_engine.cuh -- batched complex DFTs in shared memory for sm_100a.
+//
+// Conventions match FFTW 2 as used by the reference (fftwnd_one,
+// Strack/speckleTrack.c:1507-1550): unnormalised, forward = exp(-2 pi i jk/N)
+// (DIR = -1), backward = exp(+2 pi i jk/N) (DIR = +1).
+//
+// A length-N line (N = N1 * N2) is transformed in place in two steps
+// (the "four-step" factorisation, x index n = N2*n1 + n2, X index
+// k = k1 + N1*k2):
+//   step 1: for every (line, n2): radix-N1 DFT over n1 in registers, times the
+//           twiddle W_N^{n2 k1}, stored back to the same slots;
+//   step 2: for every (line, k1): radix-N2 DFT over the N2 contiguous slots,
+//           held in registers until every thread has loaded, then stored to
+//           natural order k1 + N1*k2.
+// Threads are mapped line-fastest, so with an odd row stride (N+1 float2) or
+// unit line stride (column passes) every access pattern is bank-conflict free.
+//
+// Register DFTs of composite size R are built at compile time by splitting off
+// the smallest prime factor; prime factors use the direct sum.  Twiddles come
+// from a table W_TN^e = exp(-2 pi i e/TN), e < TN, read with compile-time
+// indices (uniform across the warp, so broadcast); factors of +-1, +-i are
+// applied without a multiply.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace sbfft {
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b)
+{
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cconjmul(float2 a, float2 b)  // a * conj(b)
+{
+    return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+
+constexpr int smallest_factor(int n)
+{
+    for (int p = 2; p * p <= n; ++p)
+        if (n % p == 0) return p;
+    return n;
+}
+
+// v * W_TN^{E} for the direction DIR (W = exp(DIR * 2 pi i / TN)); E reduced mod TN.
+template <int E, int TN, int DIR>
+__device__ __forceinline__ float2 twmul(float2 v, const float2* __restrict__ tw)
+{
+    constexpr int e = ((E % TN) + TN) % TN;
+    if constexpr (e == 0) {
+        return v;
+    } else if constexpr (4 * e == 2 * TN) {
+        return make_float2(-v.x, -v.y);
+    } else if constexpr (4 * e == TN) {
+        // exp(DIR * i pi/2) = DIR * i
+        return DIR > 0 ? make_float2(-v.y, v.x) : make_float2(v.y, -v.x);
+    } else if constexpr (4 * e == 3 * TN) {
+        return DIR > 0 ? make_float2(v.y, -v.x) : make_float2(-v.y, v.x);
+    } else {
+        float2 w = tw[e];  // table holds the forward (DIR=-1) twiddle
+        if (DIR > 0) w.y = -w.y;
+        return cmul(v, w);
+    }
+}
+
+// Runtime-index twiddle multiply (inter-step twiddles).
+template <int DIR>
+__device__ __forceinline__ float2 twmul_rt(float2 v, const float2* __restrict__ tw, int e)
+{
+    float2 w = tw[e];
+    if (DIR > 0) w.y = -w.y;
+    return cmul(v, w);
+}
+
+// ---------------------------------------------------------------- register DFT
+template <int R, int DIR, int TN>
+struct RegDFT {
+    static_assert(TN % R == 0, "twiddle table size must be a multiple of R");
+    static constexpr int P = (R % 4 == 0 && R > 4) ? 4 : smallest_factor(R);  // radix 4 first
+    static constexpr int M = R / P;
+
+    template <int Q, int K>
+    __device__ __forceinline__ static float2 sub_tw(float2 v, const float2* tw)
+    {
+        return twmul<Q * K * (TN / R), TN, DIR>(v, tw);
+    }
+
+    // direct P-point DFT of t[] into out[r] (prime P)
+    template <int Pp>
+    __device__ __forceinline__ static void small_dft(float2 (&t)[Pp], float2 (&o)[Pp], const float2* tw)
+    {
+        if constexpr (Pp == 2) {
+            o[0] = cadd(t[0], t[1]);
+            o[1] = csub(t[0], t[1]);
+        } else if constexpr (Pp == 4) {
+            float2 a0 = cadd(t[0], t[2]), a1 = csub(t[0], t[2]);
+            float2 b0 = cadd(t[1], t[3]), b1 = csub(t[1], t[3]);
+            float2 jb1 = DIR > 0 ? make_float2(-b1.y, b1.x) : make_float2(b1.y, -b1.x);
+            o[0] = cadd(a0, b0);
+            o[2] = csub(a0, b0);
+            o[1] = cadd(a1, jb1);
+            o[3] = csub(a1, jb1);
+        } else {
+#pragma unroll
+            for (int r = 0; r < Pp; ++r) o[r] = t[0];
+            small_dft_acc<Pp, 1>(t, o, tw);
+        }
+    }
+    template <int Pp, int Q>
+    __device__ __forceinline__ static void small_dft_acc(float2 (&t)[Pp], float2 (&o)[Pp], const float2* tw)
+    {
+        if constexpr (Q < Pp) {
+            small_dft_acc_r<Pp, Q, 0>(t, o, tw);
+            small_dft_acc<Pp, Q + 1>(t, o, tw);
+        }
+    }
+    template <int Pp, int Q, int Rr>
+    __device__ __forceinline__ static void small_dft_acc_r(float2 (&t)[Pp], float2 (&o)[Pp], const float2* tw)
+    {
+        if constexpr (Rr < Pp) {
+            o[Rr] = cadd(o[Rr], twmul<((Q * Rr) % Pp) * (TN / Pp), TN, DIR>(t[Q], tw));
+            small_dft_acc_r<Pp, Q, Rr + 1>(t, o, tw);
+        }
+    }
+
+    template <int K>
+    __device__ __forceinline__ static void combine(float2 (&sub)[P][M], float2 (&v)[R], const float2* tw)
+    {
+        if constexpr (K < M) {
+            float2 t[P], o[P];
+            t[0] = sub[0][K];
+            combine_tw<K, 1>(sub, t, tw);
+            small_dft<P>(t, o, tw);
+#pragma unroll
+            for (int r = 0; r < P; ++r) v[K + M * r] = o[r];
+            combine<K + 1>(sub, v, tw);
+        }
+    }
+    template <int K, int Q>
+    __device__ __forceinline__ static void combine_tw(float2 (&sub)[P][M], float2 (&t)[P], const float2* tw)
+    {
+        if constexpr (Q < P) {
+            t[Q] = sub_tw<Q, K>(sub[Q][K], tw);
+            combine_tw<K, Q + 1>(sub, t, tw);
+        }
+    }
+
+    __device__ __forceinline__ static void run(float2 (&v)[R], const float2* __restrict__ tw)
+    {
+        if constexpr (R == 1) {
+            return;
+        } else if constexpr (R == 4) {
+            float2 o[4];
+            small_dft<4>(v, o, tw);
+#pragma unroll
+            for (int r = 0; r < 4; ++r) v[r] = o[r];
+        } else if constexpr (P == R) {
+            float2 o[R];
+            small_dft<R>(v, o, tw);
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[r] = o[r];
+        } else {
+            float2 sub[P][M];
+#pragma unroll
+            for (int q = 0; q < P; ++q)
+#pragma unroll
+                for (int t = 0; t < M; ++t) sub[q][t] = v[q + P * t];
+#pragma unroll
+            for (int q = 0; q < P; ++q) RegDFT<M, DIR, TN>::run(sub[q], tw);
+            combine<0>(sub, v, tw);
+        }
+    }
+};
+
+// ---------------------------------------------------------------- line FFTs
+// Lines are addressed as base + (l % NLI) * LS + (l / NLI) * IS (NLI lines per
+// image, several images side by side).  Element k of a line is at k * ES.
+template <int N1, int N2, int DIR, int NL, int NLI, int NT>
+__device__ __forceinline__ void fft_lines(float2* base, int LS, int ES, int IS, const float2* __restrict__ tw)
+{
+    constexpr int N = N1 * N2;
+    constexpr int T1 = NL * N2;
+    constexpr int R1 = (T1 + NT - 1) / NT;
+    const int tid = threadIdx.x;
+#pragma unroll
+    for (int r = 0; r < R1; ++r) {
+        const int t = tid + r * NT;
+        if (T1 % NT == 0 || t < T1) {
+            const int l = t % NL, n2 = t / NL;
+            float2* p = base + (l % NLI) * LS + (l / NLI) * IS + n2 * ES;
+            float2 v[N1];
+#pragma unroll
+            for (int n1 = 0; n1 < N1; ++n1) v[n1] = p[(N2 * n1) * ES];
+            RegDFT<N1, DIR, N>::run(v, tw);
+#pragma unroll
+            for (int k1 = 1; k1 < N1; ++k1) v[k1] = twmul_rt<DIR>(v[k1], tw, (k1 * n2) % N);
+#pragma unroll
+            for (int k1 = 0; k1 < N1; ++k1) p[(N2 * k1) * ES] = v[k1];
+        }
+    }
+    __syncthreads();
+    constexpr int T2 = NL * N1;
+    constexpr int R2 = (T2 + NT - 1) / NT;
+    float2 v2[R2][N2];
+#pragma unroll
+    for (int r = 0; r < R2; ++r) {
+        const int t = tid + r * NT;
+        if (T2 % NT == 0 || t < T2) {
+            const int l = t % NL, k1 = t / NL;
+            const float2* p = base + (l % NLI) * LS + (l / NLI) * IS + (N2 * k1) * ES;
+#pragma unroll
+            for (int n2 = 0; n2 < N2; ++n2) v2[r][n2] = p[n2 * ES];
+            RegDFT<N2, DIR, N>::run(v2[r], tw);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < R2; ++r) {
+        const int t = tid + r * NT;
+        if (T2 % NT == 0 || t < T2) {
+            const int l = t % NL, k1 = t / NL;
+            float2* p = base + (l % NLI) * LS + (l / NLI) * IS + k1 * ES;
+#pragma unroll
+            for (int k2 = 0; k2 < N2; ++k2) p[(N1 * k2) * ES] = v2[r][k2];
+        }
+    }
+    __syncthreads();
+}
+
+// Factorisation used for each supported transform length.
+template <int N>
+struct Split;
+template <> struct Split<8>   { static constexpr int N1 = 2,  N2 = 4;  };
+template <> struct Split<16>  { static constexpr int N1 = 4,  N2 = 4;  };
+template <> struct Split<24>  { static constexpr int N1 = 3,  N2 = 8;  };
+template <> struct Split<32>  { static constexpr int N1 = 4,  N2 = 8;  };
+template <> struct Split<48>  { static constexpr int N1 = 6,  N2 = 8;  };
+template <> struct Split<64>  { static constexpr int N1 = 8,  N2 = 8;  };
+template <> struct Split<96>  { static constexpr int N1 = 6,  N2 = 16; };
+template <> struct Split<128> { static constexpr int N1 = 8,  N2 = 16; };
+template <> struct Split<192> { static constexpr int N1 = 12, N2 = 16; };
+template <> struct Split<224> { static constexpr int N1 = 14, N2 = 16; };
+template <> struct Split<256> { static constexpr int N1 = 16, N2 = 16; };
+template <> struct Split<384> { static constexpr int N1 = 24, N2 = 16; };
+template <> struct Split<448> { static constexpr int N1 = 28, N2 = 16; };
+template <> struct Split<512> { static constexpr int N1 = 32, N2 = 16; };
+
+// 2-D transform of NIMG row-major N x N images in shared memory (row stride
+// RS float2, image stride IS float2): rows (range) then columns (azimuth).
+template <int N, int DIR, int NIMG, int NT>
+__device__ __forceinline__ void fft2d_smem(float2* base, int RS, int IS, const float2* __restrict__ tw)
+{
+    constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
+    fft_lines<N1, N2, DIR, N * NIMG, N, NT>(base, RS, 1, IS, tw);  // rows: line = row
+    fft_lines<N1, N2, DIR, N * NIMG, N, NT>(base, 1, RS, IS, tw);  // columns: line = column
+}
+
+// 2-D transform of an N x N row-major array anywhere in memory (row stride N;
+// normally a per-CTA global workspace that stays in L2), staged through a
+// shared tile of G lines of N+1 float2: rows first, then columns.
+template <int N, int DIR, int NT>
+__device__ __forceinline__ void fft2d_staged(float2* g, float2* tile, const float2* __restrict__ tw)
+{
+    constexpr int G = (N % 16 == 0) ? 16 : 8;
+    constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
+    const int tid = threadIdx.x;
+    for (int r0 = 0; r0 < N; r0 += G) {
+        for (int e = tid; e < G * N; e += NT) {
+            const int l = e / N, k = e % N;
+            tile[l * (N + 1) + k] = g[(size_t)(r0 + l) * N + k];
+        }
+        __syncthreads();
+        fft_lines<N1, N2, DIR, G, G, NT>(tile, N + 1, 1, 0, tw);
+        for (int e = tid; e < G * N; e += NT) {
+            const int l = e / N, k = e % N;
+            g[(size_t)(r0 + l) * N + k] = tile[l * (N + 1) + k];
+        }
+        __syncthreads();
+    }
+    for (int c0 = 0; c0 < N; c0 += G) {
+        for (int e = tid; e < N * G; e += NT) {
+            const int k = e / G, l = e % G;
+            tile[k * (G + 1) + l] = g[(size_t)k * N + c0 + l];
+        }
+        __syncthreads();
+        fft_lines<N1, N2, DIR, G, G, NT>(tile, 1, G + 1, 0, tw);
+        for (int e = tid; e < N * G; e += NT) {
+            const int k = e / G, l = e % G;
+            g[(size_t)k * N + c0 + l] = tile[k * (G + 1) + l];
+        }
+        __syncthreads();
+    }
+}
+
+template <int N>
+struct StagedTile {
+    static constexpr int G = (N % 16 == 0) ? 16 : 8;
+    static constexpr int elems = (G * (N + 1) > N * (G + 1)) ? G * (N + 1) : N * (G + 1);
+};
+
+}  // namespace sbfft

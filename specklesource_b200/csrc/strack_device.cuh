@@ -1,0 +1,338 @@
+// strack_device.cuh -- device helpers shared by the strack stage kernels:
+// block reductions, the fftshift argmax of findCPeak, the 8x8 -> 96x96
+// oversampling window, and the Levenberg-Marquardt 1-D Gaussian peak fit.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "fft_engine.cuh"
+#include "strack_common.cuh"
+
+namespace sbk {
+
+constexpr int OSW = 48;  // oversampled search window: rows/cols [24, 72) of 96
+
+__device__ __forceinline__ double warp_allsum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Sum K doubles over the block; every thread gets the totals.
+// red: shared scratch of (NT/32)*K doubles.
+template <int K, int NT>
+__device__ __forceinline__ void block_allsum(double (&v)[K], double* red)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = warp_allsum(v[k]);
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) red[warp * K + k] = v[k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < NT / 32; ++w) s += red[w * K + k];
+        v[k] = s;
+    }
+    __syncthreads();
+}
+
+// (value, rank) maximum: larger value wins, equal values -> smaller rank.
+struct ArgMax {
+    float v;
+    int rank;
+    int pos;
+};
+__device__ __forceinline__ bool am_better(float v, int rank, float bv, int brank)
+{
+    return v > bv || (v == bv && rank < brank);
+}
+__device__ __forceinline__ ArgMax warp_argmax(ArgMax a)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        float v = __shfl_xor_sync(0xffffffffu, a.v, o);
+        int r = __shfl_xor_sync(0xffffffffu, a.rank, o);
+        int p = __shfl_xor_sync(0xffffffffu, a.pos, o);
+        if (am_better(v, r, a.v, a.rank)) {
+            a.v = v;
+            a.rank = r;
+            a.pos = p;
+        }
+    }
+    return a;
+}
+// Block argmax; all threads receive the result.  scratch: 3*(NT/32) words.
+template <int NT>
+__device__ __forceinline__ ArgMax block_argmax(ArgMax a, int* scratch)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    a = warp_argmax(a);
+    if (lane == 0) {
+        scratch[warp] = __float_as_int(a.v);
+        scratch[NT / 32 + warp] = a.rank;
+        scratch[2 * (NT / 32) + warp] = a.pos;
+    }
+    __syncthreads();
+    ArgMax b;
+    b.v = __int_as_float(scratch[0]);
+    b.rank = scratch[NT / 32];
+    b.pos = scratch[2 * (NT / 32)];
+#pragma unroll
+    for (int w = 1; w < NT / 32; ++w) {
+        float v = __int_as_float(scratch[w]);
+        int r = scratch[NT / 32 + w];
+        if (am_better(v, r, b.v, b.rank)) {
+            b.v = v;
+            b.rank = r;
+            b.pos = scratch[2 * (NT / 32) + w];
+        }
+    }
+    __syncthreads();
+    return b;
+}
+
+// Scan rank of position (y, x) of the fftshifted surface in findCPeak's loop
+// (speckleTrack.c:750-788): for each (i < h, j < h) the four quadrants are
+// visited in the order (i,j), (i+h,j+h), (i+h,j), (i,j+h).
+__device__ __forceinline__ int cpeak_rank(int y, int x, int h)
+{
+    const int yi = y >= h, xi = x >= h;
+    const int i = y - yi * h, j = x - xi * h;
+    const int q = (!yi && !xi) ? 0 : (yi && xi) ? 1 : (yi ? 2 : 3);
+    return (i * h + j) * 4 + q;
+}
+
+// 96-point oversampling as a matrix: output n (in [24,72)) of the inverse
+// 96-point DFT of the zero-padded 8-point spectrum of x[t] is
+//   sum_t A[n][t] x[t],  A[n][t] = sum_{f=-4..3} exp(+2 pi i f (n - 12 t) / 96)
+// (zeroPadFFT places bins 0..3 at 0..3 and bins 4..7, Nyquist included, at
+// 92..95; speckleTrack.c:2014-2038).  osA holds A for n = 24..71, row-major
+// [n-24][t], computed on the host in double precision.
+//
+// Evaluates the 48 x 48 window of the 2-D oversampled block
+// O = A X A^T for the 8x8 real block X (row-major in blk) and returns the
+// first maximum of |O| in row-major order (strict >, as cmpTrackFast
+// :685-699).  T: shared scratch of 8*48 float2.
+template <int NT>
+__device__ __forceinline__ ArgMax oversample_peak(const float* blk, const float2* osA, float2* T, int* scratch)
+{
+    const int tid = threadIdx.x;
+    // T[t1][n2] = sum_t2 X[t1][t2] * A[n2][t2]
+    for (int e = tid; e < NFAST * OSW; e += NT) {
+        const int t1 = e / OSW, n2 = e % OSW;
+        float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int t2 = 0; t2 < NFAST; ++t2) {
+            const float x = blk[t1 * NFAST + t2];
+            const float2 a = osA[n2 * NFAST + t2];
+            acc.x = fmaf(x, a.x, acc.x);
+            acc.y = fmaf(x, a.y, acc.y);
+        }
+        T[t1 * OSW + n2] = acc;
+    }
+    __syncthreads();
+    ArgMax best;
+    best.v = 0.f;
+    best.rank = 0x7fffffff;
+    best.pos = 0;
+    for (int e = tid; e < OSW * OSW; e += NT) {
+        const int n1 = e / OSW, n2 = e % OSW;
+        float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int t1 = 0; t1 < NFAST; ++t1) {
+            const float2 a = osA[n1 * NFAST + t1];
+            const float2 t = T[t1 * OSW + n2];
+            acc.x = fmaf(a.x, t.x, fmaf(-a.y, t.y, acc.x));
+            acc.y = fmaf(a.x, t.y, fmaf(a.y, t.x, acc.y));
+        }
+        const float v = sqrtf(acc.x * acc.x + acc.y * acc.y);
+        if (am_better(v, e, best.v, best.rank) && v > 0.f) {
+            best.v = v;
+            best.rank = e;
+            best.pos = e;
+        }
+    }
+    ArgMax r = block_argmax<NT>(best, scratch);
+    if (r.rank == 0x7fffffff) {  // nothing above 0: the reference keeps index 0,0
+        r.v = 0.f;
+        r.pos = 0;
+    }
+    return r;
+}
+
+// ---------------------------------------------------------------- LM fit
+// gaussPeak1D (speckleTrack.c:2137-2202) with mrqminMod/mrqcofMod
+// (:2309-2416) and a full-pivot Gauss-Jordan solve, in double precision.
+// One warp per fit; lanes 0..17 hold the samples (x, y).  Every lane runs the
+// 3x3 algebra redundantly on warp-reduced sums.
+
+struct LMSums {
+    double al[6];  // alpha 11, 21, 22, 31, 32, 33
+    double be[3];
+    double chisq;
+};
+
+__device__ __forceinline__ LMSums lm_cof(double x, double y, bool active, const double a[4])
+{
+    LMSums s;
+    double dyda[4] = {0, 0, 0, 0};
+    double ymod = 0.0;
+    if (active) {
+        const double sig = a[3];
+        const double t = x - a[2];
+        const double argx = 0.5 * t * t / (sig * sig);
+        const double ex = exp(-argx);
+        ymod = a[1] * ex;
+        dyda[1] = ex;
+        dyda[2] = ymod * t / (sig * sig);
+        dyda[3] = ymod * t * t / (sig * sig * sig);
+    }
+    const double sig2i = active ? 1.0 / (0.1 * 0.1) : 0.0;
+    const double dy = active ? y - ymod : 0.0;
+    const double w1 = dyda[1] * sig2i, w2 = dyda[2] * sig2i, w3 = dyda[3] * sig2i;
+    s.al[0] = w1 * dyda[1];
+    s.al[1] = w2 * dyda[1];
+    s.al[2] = w2 * dyda[2];
+    s.al[3] = w3 * dyda[1];
+    s.al[4] = w3 * dyda[2];
+    s.al[5] = w3 * dyda[3];
+    s.be[0] = dy * w1;
+    s.be[1] = dy * w2;
+    s.be[2] = dy * w3;
+    s.chisq = dy * dy * sig2i;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) s.al[k] = warp_allsum(s.al[k]);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) s.be[k] = warp_allsum(s.be[k]);
+    s.chisq = warp_allsum(s.chisq);
+    return s;
+}
+
+__device__ __forceinline__ void lm_unpack(const LMSums& s, double al[4][4], double be[4])
+{
+    al[1][1] = s.al[0];
+    al[2][1] = al[1][2] = s.al[1];
+    al[2][2] = s.al[2];
+    al[3][1] = al[1][3] = s.al[3];
+    al[3][2] = al[2][3] = s.al[4];
+    al[3][3] = s.al[5];
+    be[1] = s.be[0];
+    be[2] = s.be[1];
+    be[3] = s.be[2];
+}
+
+// Gauss-Jordan with full pivoting (3x3, one right-hand side); false if singular.
+__device__ __forceinline__ bool gaussj3(double a[4][4], double b[4])
+{
+    int indxc[4], indxr[4], ipiv[4] = {0, 0, 0, 0};
+    int irow = 1, icol = 1;
+    for (int i = 1; i <= 3; i++) {
+        double big = 0.0;
+        for (int j = 1; j <= 3; j++)
+            if (ipiv[j] != 1)
+                for (int k = 1; k <= 3; k++) {
+                    if (ipiv[k] == 0) {
+                        if (fabs(a[j][k]) >= big) {
+                            big = fabs(a[j][k]);
+                            irow = j;
+                            icol = k;
+                        }
+                    } else if (ipiv[k] > 1)
+                        return false;
+                }
+        ++(ipiv[icol]);
+        if (irow != icol) {
+            for (int l = 1; l <= 3; l++) {
+                double t = a[irow][l];
+                a[irow][l] = a[icol][l];
+                a[icol][l] = t;
+            }
+            double t = b[irow];
+            b[irow] = b[icol];
+            b[icol] = t;
+        }
+        indxr[i] = irow;
+        indxc[i] = icol;
+        if (a[icol][icol] == 0.0) return false;
+        const double pivinv = 1.0 / a[icol][icol];
+        a[icol][icol] = 1.0;
+        for (int l = 1; l <= 3; l++) a[icol][l] *= pivinv;
+        b[icol] *= pivinv;
+        for (int ll = 1; ll <= 3; ll++)
+            if (ll != icol) {
+                const double dum = a[ll][icol];
+                a[ll][icol] = 0.0;
+                for (int l = 1; l <= 3; l++) a[ll][l] -= a[icol][l] * dum;
+                b[ll] -= b[icol] * dum;
+            }
+    }
+    (void)indxr;
+    (void)indxc;
+    return true;
+}
+
+// Returns sigma = a[3]/2 of the fit (all lanes).
+__device__ __forceinline__ double gauss_peak_1d(float sample, int xpos, int lane)
+{
+    const bool active = lane < NGAUSS;
+    float mx = active ? sample : 0.f;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    const double maxC = (double)fmaxf(mx, 0.f);
+    const double x = (double)xpos;
+    const double y = active ? (double)sample / maxC : 0.0;
+    const double xc = (double)__shfl_sync(0xffffffffu, xpos, NGAUSS / 2);
+    double a[4] = {0.0, 1.0, xc, 2.0};
+    double alamda = 0.001;
+    LMSums s0 = lm_cof(x, y, active, a);
+    double alpha[4][4], beta[4];
+    lm_unpack(s0, alpha, beta);
+    double ochisq = s0.chisq;
+    double lasti = 2e9;
+    for (int it = 0; it < 5; ++it) {
+        double covar[4][4], da[4];
+        for (int j = 1; j <= 3; j++) {
+            for (int k = 1; k <= 3; k++) covar[j][k] = alpha[j][k];
+            covar[j][j] = alpha[j][j] * (1.0 + alamda);
+            da[j] = beta[j];
+        }
+        if (!gaussj3(covar, da)) break;
+        double atry[4] = {0.0, a[1] + da[1], a[2] + da[2], a[3] + da[3]};
+        LMSums s1 = lm_cof(x, y, active, atry);
+        if (s1.chisq < ochisq) {
+            alamda *= 0.1;
+            ochisq = s1.chisq;
+            lm_unpack(s1, alpha, beta);
+            a[1] = atry[1];
+            a[2] = atry[2];
+            a[3] = atry[3];
+        } else {
+            alamda *= 10.0;
+        }
+        if (fabs(a[2] - lasti) < 0.001) break;
+        lasti = a[2];
+    }
+    return a[3] * .5;
+}
+
+// Doppler roll from the lag-1 sums (estDopCarrier1, dopplerEstimation.c:25-40),
+// rescaled to wA.  A NaN angle (all-zero sums) gives roll 0.
+__device__ __forceinline__ int dop_shift(double sr1, double si1, double sr2, double si2, int nAz, int wA)
+{
+    const double PI_ = 3.14159265358979323846;
+    const double an1 = (sr1 == 0.0 && si1 == 0.0) ? nan("") : atan2(si1, sr1);
+    const double an2 = (sr2 == 0.0 && si2 == 0.0) ? nan("") : atan2(si2, sr2);
+    const double v = (double)(nAz / 2) * (an1 + an2) * .5 / PI_;
+    int shift = (v != v) ? 0 : ((v >= 0.0) ? (int)(v + 0.5) : (int)(v - 0.5));
+    if (shift < 0) shift += nAz;
+    return (int)((float)shift * (float)wA / (float)nAz);
+}
+
+}  // namespace sbk

@@ -1,0 +1,73 @@
+// strack_kernels.h -- launch interface between the C-ABI host code and the
+// strack / strackw / cull kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "strack_common.cuh"
+
+namespace sbk {
+
+// Arguments of the complex stage (one grid point per CTA iteration).
+struct CmplxArgs {
+    const void* img1;
+    const void* img2;
+    int nr1, na1, nr2, na2;
+    int sampleType, byteOrder;
+    const PointPlan* plan;
+    const int* list;
+    int nList;
+    const float* hanning;  // W x W, or nullptr when -noHanning
+    double hanCorr;        // 1.5 with Hanning, else 1.0
+    const float2* twW;     // W_W^e forward twiddles, W entries
+    const float2* tau;     // parity twiddles, W entries
+    const float2* osA;     // 48 x 8 oversampling matrix
+    float azThresh;
+    int checkAzFocus, noComplex;
+    int baseOn;
+    double Bn, Bp, dBn, dBp, dBnQ, dBpQ, lambda;
+    const double* sinThetaD;
+    const double* cosThetaD;
+    const double* overRange;
+    PointRec* rec;
+    FitJob* fit;  // one entry per list position
+};
+
+// Arguments of an amplitude try (small: s = 1, large: s = LA = 2).
+struct AmpArgs {
+    const void* img1;
+    const void* img2;
+    int nr1, na1, nr2, na2;
+    int sampleType, byteOrder;
+    const PointPlan* plan;
+    const int* list;
+    int nList;
+    int stage;   // 1 small, 2 large
+    int s;       // window scale
+    int wR, wA, wRa, wAa;
+    int nR;      // grid columns (to rebuild i, j from the point index)
+    int rStart, aStart, deltaR, deltaA;
+    int noComplex;
+    float azThresh;
+    int checkAzFocus;
+    const int* azEff;     // azShift in effect for each point (nullptr: use rec.azset)
+    const float2* twWs;   // W_Ws table (Ws = wa*s)
+    const float2* tw2Ws;  // W_{2Ws} table
+    const float2* tau;    // parity twiddles for Ws
+    const float2* osA;
+    float2* scratch;      // per-CTA workspace
+    size_t scratchPerCta; // float2 elements
+    PointRec* rec;
+    FitJob* fit;
+};
+
+bool cmplx_supported(int W);
+int cmplx_blocks_per_sm(int W);
+cudaError_t launch_strack_cmplx(int W, const CmplxArgs& a, int nCta, cudaStream_t st);
+
+bool amp_supported(int Ws);
+size_t amp_scratch_elems(int Ws);
+int amp_threads(int Ws);
+cudaError_t launch_strack_amp(int Ws, const AmpArgs& a, int nCta, cudaStream_t st);
+
+}  // namespace sbk

@@ -1,0 +1,233 @@
+"""Known-answer tests that pin the CPU oracle (the reference ships none).
+
+The reference cannot be built here and has no golden vectors, so parity is
+"unpinned"; these tests pin the oracle to properties the reference's
+algorithm must have: FFTW-convention transforms, exact recovery of integer and
+band-limited sub-pixel shifts, in-band failure values, and the cull rules on
+hand-built grids.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle
+from specklesource_b200 import abi
+
+LARGE = float(abi.SB_LARGEINT)
+
+
+def _speckle(na, nr, seed, band=0.8):
+    rng = np.random.default_rng(seed)
+    z = rng.standard_normal((na, nr)) + 1j * rng.standard_normal((na, nr))
+    Z = np.fft.fft2(z)
+    fy = np.abs(np.fft.fftfreq(na)) <= band / 2
+    fx = np.abs(np.fft.fftfreq(nr)) <= band / 2
+    z = np.fft.ifft2(Z * (fy[:, None] & fx[None, :]))
+    return z / np.sqrt(np.mean(np.abs(z) ** 2))
+
+
+def _fourier_shift(z, da, dr):
+    """z2(y, x) = z(y - da, x - dr) exactly (periodic, band-limited)."""
+    na, nr = z.shape
+    fy = np.fft.fftfreq(na)[:, None]
+    fx = np.fft.fftfreq(nr)[None, :]
+    return np.fft.ifft2(np.fft.fft2(z) * np.exp(-2j * np.pi * (fy * da + fx * dr)))
+
+
+@pytest.mark.parametrize("shape,sign", [((8, 8), -1), ((24, 32), -1), ((96, 96), 1), ((21, 21), 1), ((28, 14), -1)])
+def test_fft_matches_numpy_convention(shape, sign):
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    got = oracle.fft2d(x, sign)
+    want = np.fft.fft2(x) if sign < 0 else np.fft.ifft2(x) * x.size
+    assert np.allclose(got, want, rtol=1e-12, atol=1e-10)
+
+
+def _params(**kw):
+    base = dict(rStart=48, aStart=48, deltaR=16, deltaA=16, nR=10, nA=10, wR=32, wA=32, wRa=32, wAa=32)
+    base.update(kw)
+    return abi.TrackParams(**base)
+
+
+@pytest.mark.parametrize("dr,da", [(3, -2), (-5, 4), (0, 0)])
+def test_integer_shift_is_recovered(dr, da):
+    z = _speckle(256, 256, 11)
+    z2 = np.roll(z, (da, dr), axis=(0, 1))
+    p = _params()
+    o = oracle.strack(p, z.astype(np.complex64), z2.astype(np.complex64))
+    assert (o["type"] == abi.SB_CMATCH).all()
+    # offsets are multiples of the 1/24 px quantum; an exact shift lands within one
+    assert np.abs(o["offR"] - dr).max() <= 1 / 24 + 1e-6
+    assert np.abs(o["offA"] - da).max() <= 1 / 24 + 1e-6
+    assert (o["corr"] > 0.9).all()
+
+
+@pytest.mark.parametrize("dr,da", [(1.25, -0.5), (-2.4, 0.3), (0.7, 1.9)])
+def test_subpixel_shift_within_quantum(dr, da):
+    z = _speckle(256, 256, 12)
+    z2 = _fourier_shift(z, da, dr)
+    p = _params()
+    o = oracle.strack(p, z.astype(np.complex64), z2.astype(np.complex64))
+    assert (o["type"] == abi.SB_CMATCH).all()
+    assert np.median(np.abs(o["offR"] - dr)) <= 1 / 24
+    assert np.median(np.abs(o["offA"] - da)) <= 1 / 24
+    assert np.abs(o["offR"] - dr).max() <= 2 / 24
+
+
+def test_amplitude_only_tracks_shift():
+    z = _speckle(256, 256, 13)
+    z2 = _fourier_shift(z, 0.5, 2.25)
+    p = _params(noComplex=1)
+    o = oracle.strack(p, z.astype(np.complex64), z2.astype(np.complex64))
+    assert (o["type"] == abi.SB_AMPMATCH).all()
+    assert np.median(np.abs(o["offR"] - 2.25)) < 0.1
+    assert np.median(np.abs(o["offA"] - 0.5)) < 0.1
+
+
+def test_zero_patch_fails_in_band():
+    z = _speckle(256, 256, 14)
+    z2 = z.copy()
+    z[:128, :] = 0
+    z2[:128, :] = 0
+    p = _params()
+    o = oracle.strack(p, z.astype(np.complex64), z2.astype(np.complex64))
+    top = o["type"][:3]  # grid rows whose windows lie in the zeroed half
+    assert (top == abi.SB_BAD).all()
+    assert (o["offR"][:3] == -LARGE).all() and (o["offA"][:3] == -LARGE).all()
+    assert (o["corr"][:3] == 0).all()
+    assert (o["type"][-3:] == abi.SB_CMATCH).all()
+
+
+def test_out_of_bounds_points_are_bad():
+    z = _speckle(128, 128, 15)
+    p = _params(rStart=0, aStart=0, nR=3, nA=3)  # first row/col windows start at -16
+    o = oracle.strack(p, z.astype(np.complex64), z.astype(np.complex64))
+    assert (o["type"][0, :] == abi.SB_BAD).all() and (o["type"][:, 0] == abi.SB_BAD).all()
+    assert o["stats"]["nAttempted"] == 9
+
+
+def test_big_endian_input_is_identical():
+    z = _speckle(128, 128, 16).astype(np.complex64)
+    z2 = np.roll(z, (1, 2), axis=(0, 1))
+    p = _params(rStart=40, aStart=40, nR=4, nA=4)
+    a = oracle.strack(p, z, z2)
+    b = oracle.strack(p, z.astype(">c8"), z2.astype(">c8"))
+    for k in ("offR", "offA", "corr", "type", "azd"):
+        assert np.array_equal(a[k], b[k])
+
+
+def test_f32_oracle_agrees_with_f64(small_pair_np):
+    a, b = small_pair_np
+    p = _params(rStart=40, aStart=40, nR=28, nA=28, deltaR=16, deltaA=8)
+    o64 = oracle.strack(p, a, b, precision="f64")
+    o32 = oracle.strack(p, a, b, precision="f32")
+    ok = o64["type"] > 0
+    assert (o64["type"] == o32["type"]).mean() >= 0.99
+    d = np.abs(o64["offR"] - o32["offR"])[ok & (o32["type"] > 0)]
+    assert (d <= 0.01).mean() >= 0.99
+
+
+def test_doppler_roll_of_a_carrier():
+    # a pure azimuth carrier exp(2 pi i f y) gives roll round(nAz/2 * 2 f)
+    na = nr = 32
+    y = np.arange(na)[:, None] * np.ones((1, nr))
+    rng = np.random.default_rng(3)
+    for f in (0.05, 0.2, -0.15):
+        z = np.exp(2j * np.pi * f * y) * (1 + 0.01 * rng.standard_normal((na, nr)))
+        s = oracle.est_dop_carrier(z, z, na)
+        want = int(np.floor(na / 2 * 2 * f + 0.5)) if f >= 0 else int(np.ceil(na / 2 * 2 * f - 0.5))
+        if want < 0:
+            want += na
+        assert s == want
+
+
+# ---------------------------------------------------------------- cull
+
+
+def _grid(nA=30, nR=40, seed=0):
+    rng = np.random.default_rng(seed)
+    yy, xx = np.mgrid[0:nA, 0:nR]
+    offR = (0.5 + 0.01 * xx + 0.005 * yy + 0.02 * rng.standard_normal((nA, nR))).astype(np.float32)
+    offA = (-0.3 + 0.004 * xx + 0.02 * rng.standard_normal((nA, nR))).astype(np.float32)
+    corr = np.full((nA, nR), 0.5, np.float32)
+    mt = np.ones((nA, nR), np.uint8)
+    return offR, offA, corr, mt
+
+
+def test_cull_removes_isolated_outlier():
+    offR, offA, corr, mt = _grid()
+    offR[10, 10] += 5.0
+    p = abi.CullParams(nR=40, nA=30, islandThresh=-1)
+    d = oracle.cull(p, offR, offA, corr, mt, passes=("st",))
+    assert d["offR"][10, 10] == -LARGE
+    assert (d["offR"][12:20, 12:20] > -LARGE).all()
+
+
+def test_cull_needs_enough_neighbours():
+    offR, offA, corr, mt = _grid()
+    p = abi.CullParams(nR=40, nA=30, nGood=17)
+    d = oracle.cull(p, offR, offA, corr, mt, passes=("st",))
+    # a 9x9 box clipped at a corner holds 25 points (> 17): kept
+    assert d["offR"][0, 0] > -LARGE
+    p = abi.CullParams(nR=40, nA=30, nGood=30)
+    d = oracle.cull(p, offR, offA, corr, mt, passes=("st",))
+    assert d["offR"][0, 0] == -LARGE and d["offR"][15, 20] > -LARGE
+
+
+def test_cull_corr_threshold():
+    offR, offA, corr, mt = _grid()
+    corr[5, 5] = 0.05
+    p = abi.CullParams(nR=40, nA=30, corrThresh=0.1)
+    d = oracle.cull(p, offR, offA, corr, mt, passes=("st",))
+    assert d["offR"][5, 5] == -LARGE and d["type"][5, 5] == 0
+
+
+def test_cull_nan_survives_median_pass_then_dropped():
+    offR, offA, corr, mt = _grid()
+    offR[15, 15] = np.nan
+    p = abi.CullParams(nR=40, nA=30)
+    d = oracle.cull(p, offR, offA, corr, mt, passes=("st",))
+    assert np.isnan(d["offR"][15, 15])
+    d = oracle.cull(p, offR, offA, corr, mt)
+    assert d["offRS"][15, 15] == -LARGE
+    assert d["sigmaA"][15, 15] == -LARGE
+
+
+def test_cull_smoothing_weights():
+    nA, nR = 20, 20
+    offR = np.zeros((nA, nR), np.float32)
+    offR[:, 10] = 1.0  # a column of ones
+    offA = np.zeros((nA, nR), np.float32)
+    corr = np.ones((nA, nR), np.float32)
+    mt = np.ones((nA, nR), np.uint8)
+    p = abi.CullParams(nR=nR, nA=nA, sR=2, sA=1, nGood=0, maxA=10, maxR=10)
+    d = oracle.cull(p, offR, offA, corr, mt, passes=("stats", "smooth"))
+    # weights 0.5, 1, 0.5 across range: neighbours of the column see 0.5/2
+    assert d["offRS"][10, 10] == pytest.approx(1.0 / 2.0)
+    assert d["offRS"][10, 9] == pytest.approx(0.5 / 2.0)
+
+
+def test_cull_islands_by_extent_and_last_label():
+    nA, nR = 30, 30
+    offRS = np.full((nA, nR), -LARGE, np.float32)
+    offRS[2:5, 2:5] = 1.0      # island A, extent 2 (first label)
+    offRS[10:25, 10:25] = 1.0  # big region, extent 14
+    offRS[27:29, 27:29] = 1.0  # island C, extent 1 (last label: never culled)
+    d = {"offRS": offRS}
+    p = abi.CullParams(nR=nR, nA=nA, islandThresh=5)
+    r = oracle.cull(p, offRS.copy(), offRS.copy(), np.ones((nA, nR)), np.ones((nA, nR), np.uint8),
+                    passes=())
+    r["offRS"][:] = offRS
+    r["offAS"][:] = offRS
+    from oracle.oracle import _cull_data, lib
+    import ctypes as C
+    dd, cd = _cull_data(offRS, offRS, np.ones((nA, nR)), np.ones((nA, nR)))
+    dd["offRS"][:] = offRS
+    dd["offAS"][:] = offRS
+    cp = p.to_c()
+    lib("f64").oracle_cull_islands(C.byref(cp), C.byref(cd))
+    out = dd["offRS"]
+    assert (out[2:5, 2:5] == -LARGE).all()
+    assert (out[10:25, 10:25] == 1.0).all()
+    assert (out[27:29, 27:29] == 1.0).all()
+    assert cd.nIslands == 1
+    del d, r

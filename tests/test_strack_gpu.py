@@ -1,0 +1,143 @@
+"""strack on the GPU (through the C ABI) against the FP64 oracle."""
+import numpy as np
+import pytest
+
+from oracle import oracle
+from specklesource_b200 import abi, synth
+
+from .parity import compare_track
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from specklesource_b200 import build, runtime
+    build.build()
+    c = runtime.Context(0)
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="module")
+def pair_1k():
+    s1, s2 = synth.small_pair(na=1024, nr=2048)
+    return synth.to_numpy(s1), synth.to_numpy(s2)
+
+
+def _p(**kw):
+    base = dict(rStart=40, aStart=40, deltaR=16, deltaA=8, nR=27, nA=25, wR=32, wA=32, wRa=32, wAa=32)
+    base.update(kw)
+    return abi.TrackParams(**base)
+
+
+def _check(ctx, p, a, b, **kw):
+    g = ctx.strack(p, a, b)
+    o = oracle.strack(p, a, b)
+    st = compare_track(g, o, **kw)
+    print(st, g["stats"], o["stats"])
+    assert st["pass"], st
+    return g, o, st
+
+
+def test_complex_default_small(ctx, small_pair_np):
+    a, b = small_pair_np
+    g, o, st = _check(ctx, _p(), a, b)
+    assert st["n_match_oracle"] > 500
+    assert ctx.launch_count() >= 3
+
+
+def test_config1_full_grid(ctx, pair_1k):
+    a, b = pair_1k
+    p = _p(nR=124, nA=119)
+    g, o, st = _check(ctx, p, a, b)
+    for k in ("nComplex", "nAmp", "nAmpL"):
+        assert abs(g["stats"][k] - o["stats"][k]) <= max(2, 0.005 * o["stats"]["nAttempted"])
+    ok = (g["type"] > 0) & (o["type"] > 0)
+    azd_rel = np.abs(g["azd"][ok] - o["azd"][ok]) / np.abs(o["azd"][ok])
+    assert np.percentile(azd_rel, 99) < 1e-2
+
+
+def test_amplitude_only(ctx, small_pair_np):
+    a, b = small_pair_np
+    g, o, st = _check(ctx, _p(noComplex=1), a, b)
+    assert (o["type"] == abi.SB_AMPMATCH).sum() > 300
+
+
+def test_no_hanning_single_amp(ctx, small_pair_np):
+    a, b = small_pair_np
+    _check(ctx, _p(hanningFlag=0, maxTries=1), a, b)
+
+
+def test_window_64(ctx, pair_1k):
+    a, b = pair_1k
+    p = _p(wR=64, wA=64, wRa=64, wAa=64, deltaR=24, deltaA=24, nR=40, nA=20, rStart=64, aStart=64)
+    _check(ctx, p, a, b)
+
+
+def test_low_coherence_exercises_fallbacks(ctx):
+    s1, s2 = synth.make_pair(512, 512, 21, dr=lambda y, x: 1.3 + 0 * x, da=lambda y, x: -0.6 + 0 * y,
+                             coherence=0.25)
+    a, b = synth.to_numpy(s1), synth.to_numpy(s2)
+    p = _p(rStart=72, aStart=72, nR=24, nA=24, deltaR=16, deltaA=16)
+    g, o, st = _check(ctx, p, a, b)
+    assert o["stats"]["nAmp"] + o["stats"]["nAmpL"] > 0
+
+
+def test_big_endian_and_int16_inputs(ctx, small_pair_np):
+    a, b = small_pair_np
+    p = _p()
+    g1 = ctx.strack(p, a, b)
+    g2 = ctx.strack(p, a.astype(">c8"), b.astype(">c8"))
+    for k in ("offR", "offA", "corr", "type"):
+        assert np.array_equal(g1[k], g2[k])
+    scale = 3000.0
+    ai = np.stack([np.round(a.real * scale), np.round(a.imag * scale)], -1).astype(np.int16)
+    bi = np.stack([np.round(b.real * scale), np.round(b.imag * scale)], -1).astype(np.int16)
+    gi = ctx.strack(p, ai, bi)
+    oi = oracle.strack(p, ai, bi)
+    st = compare_track(gi, oi)
+    assert st["pass"], st
+    gm = ctx.strack(p, ai.astype(">i2"), bi.astype(">i2"))
+    assert np.array_equal(gm["offR"], gi["offR"])
+
+
+def test_mask_and_offset_grid(ctx, small_pair_np):
+    a, b = small_pair_np
+    rng = np.random.default_rng(5)
+    mask = (rng.random((16, 32)) > 0.3).astype(np.uint8)
+    grid = {"nr": 20, "na": 12, "r0": 0.0, "a0": 0.0, "deltaR": 32.0, "deltaA": 32.0,
+            "dr": np.full((12, 20), 2.0, np.float32), "da": np.full((12, 20), 0.4, np.float32)}
+    grid["dr"][3:5, 3:6] = -2e9  # holes: the reference keeps the previous point's r2/a2
+    p = _p(mask={"r0": 0, "a0": 0, "nr": 32, "na": 16, "nrl": 16, "nal": 16, "mask": mask},
+           polyShift=0, initOffsets=grid)
+    g, o, st = _check(ctx, p, a, b)
+    assert (o["type"] == 0).sum() > 50
+
+
+def test_zero_region_and_edges(ctx, small_pair_np):
+    a, b = small_pair_np
+    a = a.copy()
+    b = b.copy()
+    a[:96] = 0
+    b[:96] = 0
+    p = _p(rStart=0, aStart=0, nR=33, nA=33)
+    g, o, st = _check(ctx, p, a, b)
+    assert g["stats"]["nAttempted"] == o["stats"]["nAttempted"]
+
+
+def test_device_resident_inputs(ctx, small_pair_np):
+    import torch
+    a, b = small_pair_np
+    p = _p()
+    ta = torch.from_numpy(a).cuda()
+    tb = torch.from_numpy(b).cuda()
+    out = {k: torch.zeros((p.nA, p.nR), dtype=torch.float32, device="cuda") for k in ("offR", "offA", "corr", "azd")}
+    out["type"] = torch.zeros((p.nA, p.nR), dtype=torch.uint8, device="cuda")
+    ctx.strack(p, ta, tb, out=out)
+    g = ctx.strack(p, a, b)
+    for k in ("offR", "offA", "corr", "type"):
+        assert np.array_equal(out[k].cpu().numpy(), g[k])
