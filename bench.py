@@ -37,6 +37,14 @@ N_R = (NR - 2 * GRID["rStart"]) // GRID["deltaR"] + 1  # 993
 N_A = (NA - 2 * GRID["aStart"]) // GRID["deltaA"] + 1  # 1969
 
 
+def use_small_workload():
+    """2400 x 4800 pair of the same generator (71,217 patches): the profiling case."""
+    global NA, NR, N_R, N_A
+    NA, NR = 2400, 4800
+    N_R = (NR - 2 * GRID["rStart"]) // GRID["deltaR"] + 1
+    N_A = (NA - 2 * GRID["aStart"]) // GRID["deltaA"] + 1
+
+
 def _alg_flops_fft(n_points):
     import math
     return 5.0 * n_points * math.log2(n_points)
@@ -235,7 +243,12 @@ def main():
     ap.add_argument("--cpu-rows", type=int, default=6, help="grid rows per CPU process in the baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp32-peak", action="store_true")
+    ap.add_argument("--workload", default="large", choices=["large", "small"],
+                    help="small: 2400x4800 profiling case of the same generator")
     args = ap.parse_args()
+    if args.workload == "small":
+        use_small_workload()
     if args.impl == "reference":
         return run_reference(args)
 
@@ -292,7 +305,7 @@ def main():
     st0 = stages[-1]
     cm_ms = float(np.mean([s["cmplx_ms"] for s in stages]))
     ach_tflops = st0["n_cmplx"] * ALG_CMPLX / (cm_ms * 1e-3) / 1e12
-    fp32 = fp32_peak_tflops(torch)
+    fp32 = float("nan") if args.no_fp32_peak else fp32_peak_tflops(torch)
     peaks, src = measured_peaks()
     img_bytes = 2 * NA * NR * 8
 
@@ -333,7 +346,7 @@ def main():
             "value": value, "unit": "patches/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded speckle pair, no public dataset)",
-            "config": {"workload": "strack 12000x24000 w64 step 24x6 (1,955,217 patches, complex + amplitude "
+            "config": {"workload": f"strack {NA}x{NR} w64 step 24x6 ({n_pts:,} patches, complex + amplitude "
                                    "fallback)", "parallelism": f"replicas x{world}",
                        "l2": "inputs 4.6 GB >> 126 MB L2, no flush"},
             "e2e": e2e,
