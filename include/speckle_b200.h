@@ -252,6 +252,43 @@ int sb_cull_stats(sb_context *ctx, const sb_cull_params *p, sb_cull_data *d);
 int sb_cull_smooth(sb_context *ctx, const sb_cull_params *p, sb_cull_data *d);
 int sb_cull_islands(sb_context *ctx, const sb_cull_params *p, sb_cull_data *d);
 
+/* ------------------------------------------------------------------------ */
+/* Allocation-free amplitude correlation                                     */
+/* ------------------------------------------------------------------------ */
+
+/* No counterpart in the reference: an extra entry point of this library.
+ *
+ * For callers that must not allocate device memory while they run -- a host
+ * application that has reserved the GPU's memory up front for its own pool,
+ * or a latency-critical loop in which cudaMalloc/cudaFree would add an
+ * implicit device synchronisation.  It computes the amplitude try of strack
+ * (getAmpPatches + ampMatch + ampTrackFast, Strack/speckleTrack.c:398-597,
+ * 1006-1189, without the Gaussian-width fit) for nPatch pairs of wa x wa
+ * patches that the caller has already cut out, and allocates nothing: its
+ * workspace is a fixed SB_NOALLOC_SCRATCH_BYTES array in the library's device
+ * memory, which every GPU that loads the library holds until the process
+ * exits.
+ *
+ * All pointers are device pointers.  patches1/patches2: nPatch patches of
+ * wa x wa complex float32 (re, im interleaved, native byte order), patch k at
+ * offset k*wa*wa*2 floats.  azShift: per-patch spectral roll in rows
+ * (0 <= roll < wa), or NULL to estimate it from each pair as estDopCarrier1
+ * does.  Outputs per patch: haveData (1 when the zero-count and empty-patch
+ * tests pass), cMax (normalised correlation; -1 when the peak is too close
+ * to the edge), iMax/jMax (peak in 1/NOVER-sample units, or -1000).
+ * wa must be 16, 24, 32, 48 or 64 (SB_NOALLOC_MAX_WA); larger windows are
+ * rejected with SB_ERR_ARG.  The first call on a device looks up the
+ * workspace address for that device, so make it before any stream capture.
+ * Every call shares the one workspace: calls that overlap on the GPU (other
+ * threads, other contexts on the same device) race and must be serialised by
+ * the caller.  The workspace keeps the last call's contents; every element is
+ * written before it is read, so nothing needs clearing. */
+#define SB_NOALLOC_MAX_WA 64
+#define SB_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
+int sb_amp_match_noalloc(sb_context *ctx, const float *patches1, const float *patches2, int32_t nPatch,
+                         int32_t wa, const int32_t *azShift, double *cMax, int32_t *iMax, int32_t *jMax,
+                         int32_t *haveData);
+
 #ifdef __cplusplus
 }
 #endif

@@ -34,6 +34,7 @@ SIGNATURES = {
     "sb_cull_stats": (C.c_int, [_P, C.POINTER(abi.SbCullParams), C.POINTER(abi.SbCullData)]),
     "sb_cull_smooth": (C.c_int, [_P, C.POINTER(abi.SbCullParams), C.POINTER(abi.SbCullData)]),
     "sb_cull_islands": (C.c_int, [_P, C.POINTER(abi.SbCullParams), C.POINTER(abi.SbCullData)]),
+    "sb_amp_match_noalloc": (C.c_int, [_P, _P, _P, C.c_int32, C.c_int32, _P, _P, _P, _P, _P]),
 }
 
 _lib = None
