@@ -105,6 +105,7 @@ int oracle_cull_st_data(const sb_cull_params *p, sb_cull_data *d)
             size_t k = (size_t)i * nR + j;
             if (ngood > (uint32_t)p->nGood) {
                 uint32_t midIndex = ngood / 2; /* 1-based rank */
+                if (midIndex < 1) midIndex = 1; /* ngood == 1 (nGood 0): the reference reads arr[0], unset */
                 qsort(listR, ngood, sizeof(float), cmpf);
                 qsort(listA, ngood, sizeof(float), cmpf);
                 float medianR = listR[midIndex - 1], medianA = listA[midIndex - 1];

@@ -10,8 +10,3 @@ extern "C" int sb_est_dop_carrier(sb_context* c, const float*, const float*, int
 {
     return sb_ctx_fail(c, SB_ERR_UNSUPPORTED, "not built yet");
 }
-extern "C" int sb_cull(sb_context* c, const sb_cull_params*, sb_cull_data*) { return sb_ctx_fail(c, SB_ERR_UNSUPPORTED, "cull not built yet"); }
-extern "C" int sb_cull_st_data(sb_context* c, const sb_cull_params*, sb_cull_data*) { return sb_ctx_fail(c, SB_ERR_UNSUPPORTED, "cull not built yet"); }
-extern "C" int sb_cull_stats(sb_context* c, const sb_cull_params*, sb_cull_data*) { return sb_ctx_fail(c, SB_ERR_UNSUPPORTED, "cull not built yet"); }
-extern "C" int sb_cull_smooth(sb_context* c, const sb_cull_params*, sb_cull_data*) { return sb_ctx_fail(c, SB_ERR_UNSUPPORTED, "cull not built yet"); }
-extern "C" int sb_cull_islands(sb_context* c, const sb_cull_params*, sb_cull_data*) { return sb_ctx_fail(c, SB_ERR_UNSUPPORTED, "cull not built yet"); }

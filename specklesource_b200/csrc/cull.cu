@@ -1,0 +1,786 @@
+// cull.cu -- the cullst passes on the GPU (Cullst/cullst.c:71-101).
+//
+//  cullSTData (cullSTData.c:13-125): the median test runs in place in raster
+//    order, so a cull changes the neighbourhoods of later points.  The GPU
+//    keeps that order exactly with a row wavefront: one warp per grid row
+//    (rows claimed in increasing order from a counter, so the row a warp waits
+//    on is always held by a running warp), each warp walks its row left to
+//    right and, before deciding column j, waits until the previous row has
+//    finished column j + bR/2 (transitively every earlier row in the box is
+//    done that far).  Both medians (the 1-based k = ngood/2 smallest of the
+//    valid neighbours, what Numerical Recipes' select returns) come from a
+//    warp-wide radix select over order-preserving float keys.  Waits are
+//    bounded: on time-out the kernel records an error and releases its row.
+//  cullStats (cullStats.c:19-144), cullSmooth (cullSmooth.c:29-103): one
+//    thread per point.  The plane fit is least squares with singular values
+//    below 1e-5 * max dropped (svdfit), via the 3x3 normal matrix's Jacobi
+//    eigen-decomposition, in double precision.
+//  cullIslands (cullIslands.c:13-198): union-find labelling (links to the
+//    smaller index, so each root is its component's first pixel in raster
+//    order), labels numbered by first appearance, bounding boxes, and the cull
+//    of components no wider or taller than islandThresh -- except the one
+//    labelled last, which the reference's loops (i < maxLabel) skip.
+#include <cuda/atomic>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "capi_internal.h"
+
+namespace sbk {
+
+constexpr float kCulled = -2.0e9f;  // (float)-LARGEINT
+constexpr float kValidLim = -2.0e9f; // (float)(1 - LARGEINT): 1 - 2e9 rounds to -2e9 in float
+
+__device__ __forceinline__ bool valid_pt(float r, float a) { return r > kValidLim && a > kValidLim; }
+
+// ---------------------------------------------------------------- pre-pass
+
+struct CullArgs {
+    float* offR;
+    float* offA;
+    const float* corr;
+    uint8_t* type;
+    const uint8_t* mask;
+    int nR, nA;
+    int bR, bA, nGood;
+    float maxA, maxR, corrThresh;
+    int singleMT;
+    int* rowCounter;
+    int* progress;
+    int* errFlag;
+    unsigned long long* nCulled;
+};
+
+__global__ void cull_prepass_kernel(CullArgs a)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.nR * a.nA) return;
+    if (a.corr[k] < a.corrThresh) {  // cullSTData.c:38-43
+        a.offR[k] = kCulled;
+        a.offA[k] = kCulled;
+        a.type[k] = 0;
+    }
+    if (a.mask) {  // :44-61 (singleMT is only honoured with a mask)
+        const unsigned char mv = a.mask[k] & 4;
+        if (mv > 0 && (signed char)a.type[k] > 2) {
+            a.offR[k] = kCulled;
+            a.offA[k] = kCulled;
+            a.type[k] = 0;
+        }
+        if (a.singleMT > 0 && (signed char)a.type[k] != a.singleMT) {
+            a.offR[k] = kCulled;
+            a.offA[k] = kCulled;
+            a.type[k] = 0;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- median pass
+
+__device__ __forceinline__ uint32_t fkey(float f)
+{
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float fkey_inv(uint32_t k)
+{
+    const uint32_t u = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+    return __uint_as_float(u);
+}
+
+// k-th smallest key (1-based) among the lane's NV keys flagged by vmask.
+template <int NV>
+__device__ __forceinline__ uint32_t warp_kth(const uint32_t (&key)[NV], uint32_t vmask, int k)
+{
+    uint32_t prefix = 0;
+    int below = 0;
+#pragma unroll 1
+    for (int bit = 31; bit >= 0; --bit) {
+        const uint32_t hi = (bit == 31) ? 0u : (0xffffffffu << (bit + 1));
+        int c = 0;
+#pragma unroll
+        for (int v = 0; v < NV; ++v)
+            c += ((vmask >> v) & 1u) && ((key[v] & hi) == prefix) && !((key[v] >> bit) & 1u);
+        c = __reduce_add_sync(0xffffffffu, c);
+        if (below + c < k)
+            below += c, prefix |= (1u << bit);
+    }
+    return prefix;
+}
+
+template <int NV>
+__global__ void cull_median_kernel(CullArgs a, long long spinLimit)
+{
+    const int lane = threadIdx.x & 31;
+    const int hA = a.bA / 2, hR = a.bR / 2;
+    const int boxW = 2 * hR + 1;
+    cuda::atomic_ref<int, cuda::thread_scope_device> ctr(*a.rowCounter);
+    unsigned long long culledHere = 0;
+    while (true) {
+        int row = 0;
+        if (lane == 0) row = ctr.fetch_add(1, cuda::memory_order_relaxed);
+        row = __shfl_sync(0xffffffffu, row, 0);
+        if (row >= a.nA) break;
+        const int i1 = row - hA > 0 ? row - hA : 0;
+        const int i2 = row + hA < a.nA - 1 ? row + hA : a.nA - 1;
+        bool timedOut = false;
+        for (int j = 0; j < a.nR; ++j) {
+            // wait for the previous row to finish column j + hR
+            if (row > 0) {
+                const int need = (j + hR + 1 < a.nR) ? j + hR + 1 : a.nR;
+                cuda::atomic_ref<int, cuda::thread_scope_device> prev(a.progress[row - 1]);
+                int ok = 1;
+                if (lane == 0) {
+                    long long spins = 0;
+                    while (prev.load(cuda::memory_order_acquire) < need) {
+                        if (++spins > spinLimit) {
+                            ok = 0;
+                            break;
+                        }
+                        __nanosleep(64);
+                    }
+                }
+                ok = __shfl_sync(0xffffffffu, ok, 0);
+                if (!ok) {
+                    timedOut = true;
+                    break;
+                }
+                (void)prev.load(cuda::memory_order_acquire);  // every lane acquires what lane 0 saw
+                __syncwarp();
+            }
+            const int j1 = j - hR > 0 ? j - hR : 0;
+            const int j2 = j + hR < a.nR - 1 ? j + hR : a.nR - 1;
+            const int rows = i2 - i1 + 1, cols = j2 - j1 + 1;
+            const int cnt = rows * cols;
+            uint32_t kr[NV], ka[NV];
+            uint32_t vm = 0;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                const int e = lane + 32 * v;
+                kr[v] = ka[v] = 0;
+                if (e < cnt) {
+                    const int ii = i1 + e / cols, jj = j1 + e % cols;
+                    const size_t q = (size_t)ii * a.nR + jj;
+                    const float r = __ldcg(&a.offR[q]), az = __ldcg(&a.offA[q]);
+                    if (valid_pt(r, az)) {
+                        vm |= 1u << v;
+                        kr[v] = fkey(r);
+                        ka[v] = fkey(az);
+                    }
+                }
+            }
+            int ngood = 0;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) ngood += (vm >> v) & 1u;
+            ngood = __reduce_add_sync(0xffffffffu, ngood);
+            const size_t c = (size_t)row * a.nR + j;
+            bool cull;
+            if ((unsigned)ngood > (unsigned)a.nGood) {
+                int mid = ngood / 2;
+                if (mid < 1) mid = 1;
+                const float medR = fkey_inv(warp_kth<NV>(kr, vm, mid));
+                const float medA = fkey_inv(warp_kth<NV>(ka, vm, mid));
+                const float oR = __ldcg(&a.offR[c]), oA = __ldcg(&a.offA[c]);
+                const double dA = (double)(oA - medA), dR = (double)(oR - medR);
+                cull = fabs(dA) > a.maxA || fabs(dR) > a.maxR;
+            } else {
+                cull = true;
+            }
+            if (lane == 0) {
+                if (cull) {
+                    a.offR[c] = kCulled;
+                    a.offA[c] = kCulled;
+                    culledHere++;
+                }
+                cuda::atomic_ref<int, cuda::thread_scope_device> mine(a.progress[row]);
+                mine.store(j + 1, cuda::memory_order_release);
+            }
+            __syncwarp();
+            (void)boxW;
+        }
+        if (timedOut) {
+            if (lane == 0) {
+                atomicExch(a.errFlag, 1);
+                cuda::atomic_ref<int, cuda::thread_scope_device> mine(a.progress[row]);
+                mine.store(a.nR, cuda::memory_order_release);
+            }
+        }
+    }
+    if (lane == 0 && culledHere) atomicAdd(a.nCulled, culledHere);
+}
+
+// ---------------------------------------------------------------- stats
+
+__device__ void jacobi3(double A[3][3], double e[3], double V[3][3])
+{
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) V[i][j] = (i == j);
+    for (int sweep = 0; sweep < 60; sweep++) {
+        const double off = fabs(A[0][1]) + fabs(A[0][2]) + fabs(A[1][2]);
+        if (off == 0.0) break;
+        for (int pq = 0; pq < 3; pq++) {
+            const int P = pq == 2 ? 1 : 0, Q = pq == 0 ? 1 : 2;
+            if (A[P][Q] == 0.0) continue;
+            const double theta = (A[Q][Q] - A[P][P]) / (2.0 * A[P][Q]);
+            const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+            const double cs = 1.0 / sqrt(t * t + 1.0), sn = t * cs;
+            for (int k = 0; k < 3; k++) {
+                const double akp = A[k][P], akq = A[k][Q];
+                A[k][P] = cs * akp - sn * akq;
+                A[k][Q] = sn * akp + cs * akq;
+            }
+            for (int k = 0; k < 3; k++) {
+                const double apk = A[P][k], aqk = A[Q][k];
+                A[P][k] = cs * apk - sn * aqk;
+                A[Q][k] = sn * apk + cs * aqk;
+            }
+            for (int k = 0; k < 3; k++) {
+                const double vkp = V[k][P], vkq = V[k][Q];
+                V[k][P] = cs * vkp - sn * vkq;
+                V[k][Q] = sn * vkp + cs * vkq;
+            }
+        }
+    }
+    for (int i = 0; i < 3; i++) e[i] = A[i][i];
+}
+
+// svdfit with basis (x0, ii, jj) over the valid points of a box
+__device__ void plane_fit(double x0, const float* off, const float* other, int nR, int i1, int i2, int j1, int j2,
+                          double coef[3])
+{
+    double AtA[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, Atb[3] = {0, 0, 0};
+    for (int ii = i1; ii <= i2; ii++)
+        for (int jj = j1; jj <= j2; jj++) {
+            const size_t q = (size_t)ii * nR + jj;
+            const float r = off[q], o = other[q];
+            if (!valid_pt(r, o)) continue;
+            const double f[3] = {x0, (double)(float)ii, (double)(float)jj};
+            for (int u = 0; u < 3; u++) {
+                Atb[u] += f[u] * (double)r;
+                for (int v = 0; v < 3; v++) AtA[u][v] += f[u] * f[v];
+            }
+        }
+    double e[3], V[3][3];
+    jacobi3(AtA, e, V);
+    double s[3], smax = 0;
+    for (int u = 0; u < 3; u++) {
+        s[u] = e[u] > 0 ? sqrt(e[u]) : 0.0;
+        smax = s[u] > smax ? s[u] : smax;
+    }
+    const double thresh = 1.0e-5 * smax;
+    coef[0] = coef[1] = coef[2] = 0.0;
+    for (int u = 0; u < 3; u++) {
+        if (s[u] < thresh || s[u] == 0.0) continue;
+        const double proj = V[0][u] * Atb[0] + V[1][u] * Atb[1] + V[2][u] * Atb[2];
+        const double w = proj / (s[u] * s[u]);
+        for (int v = 0; v < 3; v++) coef[v] += V[v][u] * w;
+    }
+}
+
+struct StatsArgs {
+    const float* offR;
+    const float* offA;
+    float* sigmaR;
+    float* sigmaA;
+    int nR, nA;
+};
+
+__global__ void cull_stats_kernel(StatsArgs a)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.nR * a.nA) return;
+    const int i = k / a.nR, j = k % a.nR;
+    const int b = 9;  // cullStats.c:38-39
+    const int i1 = i - b / 2 > 0 ? i - b / 2 : 0, i2 = i + b / 2 < a.nA - 1 ? i + b / 2 : a.nA - 1;
+    const int j1 = j - b / 2 > 0 ? j - b / 2 : 0, j2 = j + b / 2 < a.nR - 1 ? j + b / 2 : a.nR - 1;
+    unsigned ngood = 0;
+    double meanA = 0.0, meanR = 0.0;
+    for (int ii = i1; ii <= i2; ii++)
+        for (int jj = j1; jj <= j2; jj++) {
+            const size_t q = (size_t)ii * a.nR + jj;
+            if (valid_pt(a.offR[q], a.offA[q])) {
+                ngood++;
+                meanA += a.offA[q];
+                meanR += a.offR[q];
+            }
+        }
+    meanA /= (double)ngood;
+    meanR /= (double)ngood;
+    double aR[4] = {0, 0, 0, 0}, aA[4] = {0, 0, 0, 0};
+    if (ngood > 8) {
+        double c[3];
+        plane_fit((double)(float)meanR, a.offR, a.offA, a.nR, i1, i2, j1, j2, c);
+        aR[1] = c[0] * meanR;
+        aR[2] = c[1];
+        aR[3] = c[2];
+        plane_fit((double)(float)meanA, a.offA, a.offR, a.nR, i1, i2, j1, j2, c);
+        aA[1] = c[0] * meanA;
+        aA[2] = c[1];
+        aA[3] = c[2];
+    }
+    ngood = 0;
+    meanA = meanR = 0.0;
+    double varR = 0.0, varA = 0.0;
+    for (int ii = i1; ii <= i2; ii++)
+        for (int jj = j1; jj <= j2; jj++) {
+            const size_t q = (size_t)ii * a.nR + jj;
+            if (valid_pt(a.offR[q], a.offA[q])) {
+                ngood++;
+                float oR = a.offR[q], oA = a.offA[q];
+                oR = (float)((double)oR - (aR[1] + aR[2] * (float)ii + aR[3] * (float)jj));
+                oA = (float)((double)oA - (aA[1] + aA[2] * (float)ii + aA[3] * (float)jj));
+                meanA += oA;
+                meanR += oR;
+                varA += (double)(oA * oA);
+                varR += (double)(oR * oR);
+            }
+        }
+    if (ngood > 8 && a.offR[k] > kValidLim) {
+        float sA = (float)(varA / (float)(ngood - 3));
+        float sR = (float)(varR / (float)(ngood - 3));
+        sA = (float)((double)sA - meanA * meanA / (float)((ngood - 3) * ngood));
+        sR = (float)((double)sR - meanR * meanR / (float)((ngood - 3) * ngood));
+        sA = (float)(0.00001 > (double)sA ? 0.00001 : (double)sA);
+        sR = (float)(0.00001 > (double)sR ? 0.00001 : (double)sR);
+        a.sigmaA[k] = (float)sqrt((double)sA);
+        a.sigmaR[k] = (float)sqrt((double)sR);
+    } else {
+        a.sigmaA[k] = kCulled;
+        a.sigmaR[k] = kCulled;
+    }
+}
+
+// ---------------------------------------------------------------- smooth
+
+struct SmoothArgs {
+    const float* offR;
+    const float* offA;
+    const uint8_t* type;
+    float* sigmaR;
+    float* sigmaA;
+    float* offRS;
+    float* offAS;
+    int nR, nA, sR, sA;
+};
+
+__device__ __forceinline__ float sweight(int m, int s)
+{
+    const float w2 = (float)((float)s / 2.0 - 0.01);  // cullSmooth.c:10-27
+    return (m < -w2 || m > w2) ? 0.5f : 1.0f;
+}
+
+__global__ void cull_smooth_kernel(SmoothArgs a)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.nR * a.nA) return;
+    const int i = k / a.nR, j = k % a.nR;
+    const float nlooks[4] = {0.0f, 1.0f, 0.25f, 0.015f};
+    const int i1 = i - a.sA / 2 > 0 ? i - a.sA / 2 : 0, i2 = i + a.sA / 2 < a.nA - 1 ? i + a.sA / 2 : a.nA - 1;
+    const int j1 = j - a.sR / 2 > 0 ? j - a.sR / 2 : 0, j2 = j + a.sR / 2 < a.nR - 1 ? j + a.sR / 2 : a.nR - 1;
+    double ngood = 0, meanA = 0.0, meanR = 0.0;
+    float nLooksEff = 0.0f;
+    for (int ii = i1; ii <= i2; ii++) {
+        const float wa = sweight(ii - i, a.sA);
+        for (int jj = j1; jj <= j2; jj++) {
+            const size_t q = (size_t)ii * a.nR + jj;
+            if (valid_pt(a.offR[q], a.offA[q])) {
+                const double w = (double)(wa * sweight(jj - j, a.sR));
+                ngood = __dadd_rn(ngood, w);
+                nLooksEff = (float)__dadd_rn((double)nLooksEff, __dmul_rn(w, (double)nlooks[(int)(signed char)a.type[q] & 3]));
+                meanA = __dadd_rn(meanA, __dmul_rn(w, (double)a.offA[q]));
+                meanR = __dadd_rn(meanR, __dmul_rn(w, (double)a.offR[q]));
+            }
+        }
+    }
+    if (((ngood > 1) || (a.sA == 1) || (a.sR == 1)) && a.offR[k] > kValidLim && a.sigmaA[k] > kValidLim) {
+        nLooksEff = (float)((double)nLooksEff > 1. ? (double)nLooksEff : 1.);
+        a.sigmaA[k] = (float)((double)a.sigmaA[k] / sqrt((double)nLooksEff));
+        a.sigmaR[k] = (float)((double)a.sigmaR[k] / sqrt((double)nLooksEff));
+        a.offRS[k] = (float)(meanR / (float)ngood);
+        a.offAS[k] = (float)(meanA / (float)ngood);
+    } else {
+        a.offRS[k] = kCulled;
+        a.offAS[k] = kCulled;
+    }
+}
+
+// ---------------------------------------------------------------- sim offsets
+
+__global__ void cull_sim_kernel(float* offR, float* offA, const float* simR, const float* simA, int n, float sign)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    // cullst.c:109-121 with its local LARGEINT = -2e9: offA < 2e9 + 1
+    if ((double)offA[k] < (2e9 + 1) && (double)simA[k] < (2e9 + 1)) {
+        offA[k] = offA[k] + sign * simA[k];
+        offR[k] = offR[k] + sign * simR[k];
+    }
+}
+
+// ---------------------------------------------------------------- islands
+
+__device__ __forceinline__ int uf_find(int* par, int x)
+{
+    int p = par[x];
+    while (p != x) {
+        const int g = par[p];
+        if (g < p) par[x] = g;  // path halving (only towards smaller indices)
+        x = p;
+        p = par[x];
+    }
+    return x;
+}
+
+__device__ void uf_union(int* par, int a, int b)
+{
+    bool done = false;
+    while (!done) {
+        a = uf_find(par, a);
+        b = uf_find(par, b);
+        if (a == b) return;
+        if (a < b) {
+            const int t = a;
+            a = b;
+            b = t;
+        }
+        // link the larger root a under the smaller root b
+        const int old = atomicMin(&par[a], b);
+        done = (old == a);
+        a = old;
+    }
+}
+
+struct IslandArgs {
+    float* offRS;
+    float* offAS;
+    int* par;
+    int* minX;
+    int* maxX;
+    int* minY;
+    int* maxY;
+    int* lastRoot;
+    unsigned long long* counts;  // [0] islands culled, [1] points culled
+    int nR, nA, conn8, thresh;
+};
+
+__global__ void isl_init_kernel(IslandArgs a)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.nR * a.nA) return;
+    const float minRegion = (float)(-2000000000 + 1000);  // cullIslands.c:62
+    a.par[k] = a.offRS[k] >= minRegion ? k : -1;
+    a.minX[k] = a.minY[k] = 0x7fffffff;
+    a.maxX[k] = a.maxY[k] = -0x7fffffff;
+}
+
+__global__ void isl_union_kernel(IslandArgs a)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.nR * a.nA || a.par[k] < 0) return;
+    const int i = k / a.nR, j = k % a.nR;
+    if (j > 0 && a.par[k - 1] >= 0) uf_union(a.par, k, k - 1);
+    if (i > 0 && a.par[k - a.nR] >= 0) uf_union(a.par, k, k - a.nR);
+    if (a.conn8 && i > 0) {
+        if (j > 0 && a.par[k - a.nR - 1] >= 0) uf_union(a.par, k, k - a.nR - 1);
+        if (j < a.nR - 1 && a.par[k - a.nR + 1] >= 0) uf_union(a.par, k, k - a.nR + 1);
+    }
+}
+
+__global__ void isl_flatten_kernel(IslandArgs a)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.nR * a.nA || a.par[k] < 0) return;
+    int r = k;
+    while (a.par[r] != r) r = a.par[r];
+    a.par[k] = r;
+    const int i = k / a.nR, j = k % a.nR;
+    atomicMin(&a.minX[r], j);
+    atomicMax(&a.maxX[r], j);
+    atomicMin(&a.minY[r], i);
+    atomicMax(&a.maxY[r], i);
+    if (r == k) atomicMax(a.lastRoot, k);  // the component labelled last
+}
+
+__global__ void isl_cull_kernel(IslandArgs a)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.nR * a.nA || a.par[k] < 0) return;
+    const int r = a.par[k];
+    if (r == *a.lastRoot) return;
+    if ((a.maxX[r] - a.minX[r]) > a.thresh || (a.maxY[r] - a.minY[r]) > a.thresh) return;
+    a.offRS[k] = kCulled;
+    if (a.offAS) a.offAS[k] = kCulled;
+    atomicAdd(&a.counts[1], 1ull);
+    if (r == k) atomicAdd(&a.counts[0], 1ull);
+}
+
+}  // namespace sbk
+
+// ======================================================================= C ABI
+
+using namespace sbk;
+
+namespace {
+
+struct CullDev {
+    float *offR, *offA, *corr, *simR, *simA, *offRS, *offAS, *sigmaR, *sigmaA;
+    uint8_t *type, *mask;
+};
+
+int cull_check(sb_context* c, const sb_cull_params* p, const sb_cull_data* d)
+{
+    if (!c) return SB_ERR_ARG;
+    if (!p || !d) return sb_ctx_fail(c, SB_ERR_ARG, "null params or data");
+    if (p->nR <= 0 || p->nA <= 0) return sb_ctx_fail(c, SB_ERR_ARG, "empty grid");
+    if ((long long)p->nR * p->nA > (1LL << 30)) return sb_ctx_fail(c, SB_ERR_ARG, "grid too large");
+    if (!d->offR || !d->offA || !d->corr || !d->type) return sb_ctx_fail(c, SB_ERR_ARG, "null input grid");
+    if (p->bR < 0 || p->bA < 0 || (p->bR / 2 * 2 + 1) * (p->bA / 2 * 2 + 1) > 32 * 32)
+        return sb_ctx_fail(c, SB_ERR_UNSUPPORTED, "cull box larger than 32 x 32");
+    if (p->useSim && (!d->simR || !d->simA)) return sb_ctx_fail(c, SB_ERR_ARG, "useSim needs simR/simA");
+    return SB_OK;
+}
+
+#define CKC(call, what)                                              \
+    do {                                                             \
+        cudaError_t _e = (call);                                     \
+        if (_e != cudaSuccess) return sb_ctx_cuda(c, _e, what);      \
+    } while (0)
+
+// Device views of the job's grids (copies host inputs in).
+int cull_stage_in(sb_context* c, const sb_cull_params* p, sb_cull_data* d, CullDev* v)
+{
+    const size_t n = (size_t)p->nR * p->nA, fb = n * sizeof(float);
+    cudaError_t e;
+    if (d->onDevice) {
+        v->offR = d->offR; v->offA = d->offA; v->corr = (float*)d->corr; v->type = d->type;
+        v->mask = (uint8_t*)d->mask; v->simR = (float*)d->simR; v->simA = (float*)d->simA;
+        v->offRS = d->offRS; v->offAS = d->offAS; v->sigmaR = d->sigmaR; v->sigmaA = d->sigmaA;
+        if (!v->offRS) v->offRS = (float*)sb_ctx_buf(c, "c_offRS", fb, &e);
+        if (!v->offAS) v->offAS = (float*)sb_ctx_buf(c, "c_offAS", fb, &e);
+        if (!v->sigmaR) v->sigmaR = (float*)sb_ctx_buf(c, "c_sigmaR", fb, &e);
+        if (!v->sigmaA) v->sigmaA = (float*)sb_ctx_buf(c, "c_sigmaA", fb, &e);
+        return SB_OK;
+    }
+    v->offR = (float*)sb_ctx_buf(c, "c_offR", fb, &e);
+    v->offA = (float*)sb_ctx_buf(c, "c_offA", fb, &e);
+    v->corr = (float*)sb_ctx_buf(c, "c_corr", fb, &e);
+    v->type = (uint8_t*)sb_ctx_buf(c, "c_type", n, &e);
+    v->offRS = (float*)sb_ctx_buf(c, "c_offRS", fb, &e);
+    v->offAS = (float*)sb_ctx_buf(c, "c_offAS", fb, &e);
+    v->sigmaR = (float*)sb_ctx_buf(c, "c_sigmaR", fb, &e);
+    v->sigmaA = (float*)sb_ctx_buf(c, "c_sigmaA", fb, &e);
+    v->mask = d->mask ? (uint8_t*)sb_ctx_buf(c, "c_mask", n, &e) : nullptr;
+    v->simR = p->useSim ? (float*)sb_ctx_buf(c, "c_simR", fb, &e) : nullptr;
+    v->simA = p->useSim ? (float*)sb_ctx_buf(c, "c_simA", fb, &e) : nullptr;
+    if (!v->offR || !v->offA || !v->corr || !v->type || !v->offRS || !v->offAS || !v->sigmaR || !v->sigmaA ||
+        (d->mask && !v->mask) || (p->useSim && (!v->simR || !v->simA)))
+        return sb_ctx_fail(c, SB_ERR_NOMEM, "device allocation failed");
+    cudaStream_t s = c->stream;
+    CKC(cudaMemcpyAsync(v->offR, d->offR, fb, cudaMemcpyHostToDevice, s), "h2d");
+    CKC(cudaMemcpyAsync(v->offA, d->offA, fb, cudaMemcpyHostToDevice, s), "h2d");
+    CKC(cudaMemcpyAsync(v->corr, d->corr, fb, cudaMemcpyHostToDevice, s), "h2d");
+    CKC(cudaMemcpyAsync(v->type, d->type, n, cudaMemcpyHostToDevice, s), "h2d");
+    if (d->mask) CKC(cudaMemcpyAsync(v->mask, d->mask, n, cudaMemcpyHostToDevice, s), "h2d");
+    if (p->useSim) {
+        CKC(cudaMemcpyAsync(v->simR, d->simR, fb, cudaMemcpyHostToDevice, s), "h2d");
+        CKC(cudaMemcpyAsync(v->simA, d->simA, fb, cudaMemcpyHostToDevice, s), "h2d");
+    }
+    // outputs that a single pass reads (stats -> smooth -> islands)
+    if (d->sigmaR) CKC(cudaMemcpyAsync(v->sigmaR, d->sigmaR, fb, cudaMemcpyHostToDevice, s), "h2d");
+    if (d->sigmaA) CKC(cudaMemcpyAsync(v->sigmaA, d->sigmaA, fb, cudaMemcpyHostToDevice, s), "h2d");
+    if (d->offRS) CKC(cudaMemcpyAsync(v->offRS, d->offRS, fb, cudaMemcpyHostToDevice, s), "h2d");
+    if (d->offAS) CKC(cudaMemcpyAsync(v->offAS, d->offAS, fb, cudaMemcpyHostToDevice, s), "h2d");
+    return SB_OK;
+}
+
+int cull_stage_out(sb_context* c, const sb_cull_params* p, sb_cull_data* d, const CullDev* v)
+{
+    if (d->onDevice) return SB_OK;
+    const size_t n = (size_t)p->nR * p->nA, fb = n * sizeof(float);
+    cudaStream_t s = c->stream;
+    CKC(cudaMemcpyAsync(d->offR, v->offR, fb, cudaMemcpyDeviceToHost, s), "d2h");
+    CKC(cudaMemcpyAsync(d->offA, v->offA, fb, cudaMemcpyDeviceToHost, s), "d2h");
+    CKC(cudaMemcpyAsync(d->type, v->type, n, cudaMemcpyDeviceToHost, s), "d2h");
+    if (d->offRS) CKC(cudaMemcpyAsync(d->offRS, v->offRS, fb, cudaMemcpyDeviceToHost, s), "d2h");
+    if (d->offAS) CKC(cudaMemcpyAsync(d->offAS, v->offAS, fb, cudaMemcpyDeviceToHost, s), "d2h");
+    if (d->sigmaR) CKC(cudaMemcpyAsync(d->sigmaR, v->sigmaR, fb, cudaMemcpyDeviceToHost, s), "d2h");
+    if (d->sigmaA) CKC(cudaMemcpyAsync(d->sigmaA, v->sigmaA, fb, cudaMemcpyDeviceToHost, s), "d2h");
+    return SB_OK;
+}
+
+int run_st_data(sb_context* c, const sb_cull_params* p, sb_cull_data* d, const CullDev* v)
+{
+    const int n = p->nR * p->nA;
+    cudaError_t e;
+    int* ctl = (int*)sb_ctx_buf(c, "c_ctl", sizeof(int) * 4 + sizeof(unsigned long long) * 2, &e);
+    int* progress = (int*)sb_ctx_buf(c, "c_progress", sizeof(int) * (size_t)p->nA, &e);
+    if (!ctl || !progress) return sb_ctx_fail(c, SB_ERR_NOMEM, "device allocation failed");
+    CullArgs a;
+    a.offR = v->offR; a.offA = v->offA; a.corr = v->corr; a.type = v->type; a.mask = v->mask;
+    a.nR = p->nR; a.nA = p->nA; a.bR = p->bR; a.bA = p->bA; a.nGood = p->nGood;
+    a.maxA = p->maxA; a.maxR = p->maxR; a.corrThresh = p->corrThresh; a.singleMT = p->singleMT;
+    a.rowCounter = ctl;
+    a.errFlag = ctl + 1;
+    a.nCulled = (unsigned long long*)(ctl + 4);
+    a.progress = progress;
+    cudaStream_t s = c->stream;
+    CKC(cudaMemsetAsync(ctl, 0, sizeof(int) * 4 + sizeof(unsigned long long) * 2, s), "memset");
+    CKC(cudaMemsetAsync(progress, 0, sizeof(int) * (size_t)p->nA, s), "memset");
+    cull_prepass_kernel<<<(n + 255) / 256, 256, 0, s>>>(a);
+    CKC(cudaGetLastError(), "cull_prepass");
+    c->launches++;
+    // one warp per row in flight; enough warps for the wavefront depth
+    const int box = (p->bR / 2 * 2 + 1) * (p->bA / 2 * 2 + 1);
+    const int nv = (box + 31) / 32;
+    int warps = c->numSM * 32;
+    if (warps > p->nA) warps = p->nA;
+    const int threads = 128, blocks = (warps * 32 + threads - 1) / threads;
+    const long long spinLimit = 1LL << 26;  // ~4 s of 64 ns naps per wait
+    switch (nv) {
+    case 1: cull_median_kernel<1><<<blocks, threads, 0, s>>>(a, spinLimit); break;
+    case 2: cull_median_kernel<2><<<blocks, threads, 0, s>>>(a, spinLimit); break;
+    case 3: cull_median_kernel<3><<<blocks, threads, 0, s>>>(a, spinLimit); break;
+    case 4: cull_median_kernel<4><<<blocks, threads, 0, s>>>(a, spinLimit); break;
+    case 5: case 6: case 7: case 8: cull_median_kernel<8><<<blocks, threads, 0, s>>>(a, spinLimit); break;
+    case 9: case 10: case 11: case 12: case 13: case 14: case 15: case 16:
+        cull_median_kernel<16><<<blocks, threads, 0, s>>>(a, spinLimit); break;
+    default: cull_median_kernel<32><<<blocks, threads, 0, s>>>(a, spinLimit); break;
+    }
+    CKC(cudaGetLastError(), "cull_median");
+    c->launches++;
+    int hostCtl[2];
+    unsigned long long culled = 0;
+    CKC(cudaMemcpyAsync(hostCtl, ctl, sizeof(int) * 2, cudaMemcpyDeviceToHost, s), "d2h");
+    CKC(cudaMemcpyAsync(&culled, ctl + 4, sizeof(culled), cudaMemcpyDeviceToHost, s), "d2h");
+    CKC(cudaStreamSynchronize(s), "cull_median");
+    if (hostCtl[1]) return sb_ctx_fail(c, SB_ERR_TIMEOUT, "cullSTData wavefront wait timed out");
+    d->nCulled = (int64_t)culled;
+    return SB_OK;
+}
+
+int run_stats(sb_context* c, const sb_cull_params* p, const CullDev* v)
+{
+    const int n = p->nR * p->nA;
+    StatsArgs a{v->offR, v->offA, v->sigmaR, v->sigmaA, p->nR, p->nA};
+    cull_stats_kernel<<<(n + 127) / 128, 128, 0, c->stream>>>(a);
+    c->launches++;
+    return sb_ctx_cuda(c, cudaGetLastError(), "cull_stats");
+}
+
+int run_smooth(sb_context* c, const sb_cull_params* p, const CullDev* v)
+{
+    const int n = p->nR * p->nA;
+    SmoothArgs a{v->offR, v->offA, v->type, v->sigmaR, v->sigmaA, v->offRS, v->offAS, p->nR, p->nA, p->sR, p->sA};
+    cull_smooth_kernel<<<(n + 127) / 128, 128, 0, c->stream>>>(a);
+    c->launches++;
+    return sb_ctx_cuda(c, cudaGetLastError(), "cull_smooth");
+}
+
+int run_islands(sb_context* c, const sb_cull_params* p, sb_cull_data* d, const CullDev* v)
+{
+    const int n = p->nR * p->nA;
+    cudaError_t e;
+    int* ws = (int*)sb_ctx_buf(c, "c_isl", sizeof(int) * (size_t)n * 5 + 64, &e);
+    unsigned long long* cntd = (unsigned long long*)sb_ctx_buf(c, "c_isl_cnt", 4 * sizeof(unsigned long long), &e);
+    if (!ws || !cntd) return sb_ctx_fail(c, SB_ERR_NOMEM, "device allocation failed");
+    IslandArgs a;
+    a.offRS = v->offRS;
+    a.offAS = v->offAS;
+    a.par = ws;
+    a.minX = ws + (size_t)n;
+    a.maxX = ws + 2 * (size_t)n;
+    a.minY = ws + 3 * (size_t)n;
+    a.maxY = ws + 4 * (size_t)n;
+    a.lastRoot = ws + 5 * (size_t)n;
+    a.counts = cntd;
+    a.nR = p->nR;
+    a.nA = p->nA;
+    a.conn8 = p->connectivity != 4;
+    a.thresh = p->islandThresh;
+    cudaStream_t s = c->stream;
+    CKC(cudaMemsetAsync(a.lastRoot, 0xff, sizeof(int), s), "memset");
+    CKC(cudaMemsetAsync(a.counts, 0, 2 * sizeof(unsigned long long), s), "memset");
+    const int g = (n + 255) / 256;
+    isl_init_kernel<<<g, 256, 0, s>>>(a);
+    isl_union_kernel<<<g, 256, 0, s>>>(a);
+    isl_flatten_kernel<<<g, 256, 0, s>>>(a);
+    isl_cull_kernel<<<g, 256, 0, s>>>(a);
+    c->launches += 4;
+    CKC(cudaGetLastError(), "cull_islands");
+    unsigned long long cnt[2];
+    CKC(cudaMemcpyAsync(cnt, a.counts, sizeof(cnt), cudaMemcpyDeviceToHost, s), "d2h");
+    CKC(cudaStreamSynchronize(s), "cull_islands");
+    d->nIslands = (int64_t)cnt[0];
+    d->nIslandPoints = (int64_t)cnt[1];
+    return SB_OK;
+}
+
+int run_sim(sb_context* c, const sb_cull_params* p, const CullDev* v, float sign)
+{
+    const int n = p->nR * p->nA;
+    cull_sim_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(v->offR, v->offA, v->simR, v->simA, n, sign);
+    c->launches++;
+    return sb_ctx_cuda(c, cudaGetLastError(), "cull_sim");
+}
+
+template <typename F>
+int cull_entry(sb_context* c, const sb_cull_params* p, sb_cull_data* d, F body)
+{
+    int rc = cull_check(c, p, d);
+    if (rc != SB_OK) return rc;
+    c->err.clear();
+    c->launches = 0;
+    CKC(cudaSetDevice(c->device), "cudaSetDevice");
+    cudaEventRecord(c->ev[0], c->stream);
+    CullDev v;
+    if ((rc = cull_stage_in(c, p, d, &v)) != SB_OK) return rc;
+    cudaEventRecord(c->ev[1], c->stream);
+    if ((rc = body(v)) != SB_OK) return rc;
+    cudaEventRecord(c->ev[2], c->stream);
+    if ((rc = cull_stage_out(c, p, d, &v)) != SB_OK) return rc;
+    cudaEventRecord(c->ev[3], c->stream);
+    CKC(cudaStreamSynchronize(c->stream), "cull");
+    cudaEventElapsedTime(&c->timing[0], c->ev[0], c->ev[3]);
+    cudaEventElapsedTime(&c->timing[1], c->ev[0], c->ev[1]);
+    cudaEventElapsedTime(&c->timing[2], c->ev[1], c->ev[2]);
+    cudaEventElapsedTime(&c->timing[3], c->ev[2], c->ev[3]);
+    return SB_OK;
+}
+
+}  // namespace
+
+extern "C" int sb_cull(sb_context* c, const sb_cull_params* p, sb_cull_data* d)
+{
+    return cull_entry(c, p, d, [&](const CullDev& v) {
+        int rc;
+        if (p->useSim && (rc = run_sim(c, p, &v, -1.0f)) != SB_OK) return rc;
+        const int passes = p->nCullPasses > 0 ? p->nCullPasses : 3;
+        for (int k = 0; k < passes; ++k)
+            if ((rc = run_st_data(c, p, d, &v)) != SB_OK) return rc;
+        if ((rc = run_stats(c, p, &v)) != SB_OK) return rc;
+        if (p->useSim && (rc = run_sim(c, p, &v, 1.0f)) != SB_OK) return rc;
+        if ((rc = run_smooth(c, p, &v)) != SB_OK) return rc;
+        if (p->islandThresh > 0 && (rc = run_islands(c, p, d, &v)) != SB_OK) return rc;
+        return SB_OK;
+    });
+}
+
+extern "C" int sb_cull_st_data(sb_context* c, const sb_cull_params* p, sb_cull_data* d)
+{
+    return cull_entry(c, p, d, [&](const CullDev& v) { return run_st_data(c, p, d, &v); });
+}
+
+extern "C" int sb_cull_stats(sb_context* c, const sb_cull_params* p, sb_cull_data* d)
+{
+    return cull_entry(c, p, d, [&](const CullDev& v) { return run_stats(c, p, &v); });
+}
+
+extern "C" int sb_cull_smooth(sb_context* c, const sb_cull_params* p, sb_cull_data* d)
+{
+    return cull_entry(c, p, d, [&](const CullDev& v) { return run_smooth(c, p, &v); });
+}
+
+extern "C" int sb_cull_islands(sb_context* c, const sb_cull_params* p, sb_cull_data* d)
+{
+    return cull_entry(c, p, d, [&](const CullDev& v) { return run_islands(c, p, d, &v); });
+}

@@ -1,0 +1,128 @@
+"""cullst on the GPU (through the C ABI) against the oracle: keep masks and
+culled offsets bit-exact, smoothed offsets and sigmas within float tolerance."""
+import numpy as np
+import pytest
+
+from oracle import oracle
+from specklesource_b200 import abi
+
+pytestmark = pytest.mark.gpu
+
+LARGE = np.float32(-2e9)
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from specklesource_b200 import build, runtime
+    build.build()
+    c = runtime.Context(0)
+    yield c
+    c.close()
+
+
+def offsets_field(nA, nR, seed, outliers=0.08, holes=0.02):
+    """Smooth offsets with uniform +-20 px outliers, NaN holes and failed points."""
+    rng = np.random.default_rng(seed)
+    yy, xx = np.mgrid[0:nA, 0:nR].astype(np.float64)
+    offR = 3 + 2 * np.sin(xx / 37.0) * np.cos(yy / 23.0) + 0.05 * rng.standard_normal((nA, nR))
+    offA = -1 + np.cos((xx + yy) / 41.0) + 0.05 * rng.standard_normal((nA, nR))
+    m = rng.random((nA, nR)) < outliers
+    offR[m] += rng.uniform(-20, 20, m.sum())
+    offA[m] += rng.uniform(-20, 20, m.sum())
+    h = rng.random((nA, nR)) < holes
+    offR[h] = np.nan
+    offA[h] = np.nan
+    f = rng.random((nA, nR)) < 0.05
+    offR[f] = LARGE
+    offA[f] = LARGE
+    # a failed region holding small valid islands (they survive the median
+    # passes and are removed by the island pass) and one larger valid patch
+    a0, r0 = nA // 5, nR // 5
+    block = (slice(a0, a0 + 60), slice(r0, r0 + 90))
+    offR[block] = LARGE
+    offA[block] = LARGE
+    f[block] = True
+    for k, (di, dj, s) in enumerate([(5, 5, 8), (5, 40, 7), (30, 10, 9), (30, 50, 25)]):
+        isl = (slice(a0 + di, a0 + di + s), slice(r0 + dj, r0 + dj + min(s, 35)))
+        offR[isl] = 3.0 + 0.01 * k
+        offA[isl] = -1.0
+        f[isl] = False
+    corr = rng.uniform(0, 1, (nA, nR)).astype(np.float32)
+    mt = rng.integers(1, 4, (nA, nR)).astype(np.uint8)
+    mt[f] = 0
+    return offR.astype(np.float32), offA.astype(np.float32), corr, mt
+
+
+def _same(a, b):
+    return np.array_equal(a, b, equal_nan=True)
+
+
+def _check(g, o, keys_exact=("offR", "offA", "type")):
+    for k in keys_exact:
+        assert _same(g[k], o[k]), f"{k} differs at {np.argwhere(~((g[k] == o[k]) | (np.isnan(g[k]) & np.isnan(o[k]))))[:5]}"
+    for k in ("offRS", "offAS"):
+        vg, vo = g[k] > -1.9e9, o[k] > -1.9e9
+        assert np.array_equal(vg, vo), f"{k} keep mask differs"
+        assert np.allclose(g[k][vo], o[k][vo], rtol=1e-6, atol=1e-6)
+    for k in ("sigmaR", "sigmaA"):
+        vg, vo = g[k] > -1.9e9, o[k] > -1.9e9
+        assert np.array_equal(vg, vo), f"{k} validity differs"
+        assert np.allclose(g[k][vo], o[k][vo], rtol=2e-3, atol=1e-5)
+
+
+@pytest.mark.parametrize("kw", [
+    dict(),                                                          # cullst defaults
+    dict(bR=5, bA=5, nGood=12, sR=3, sA=3, islandThresh=10),          # 5x5 median, 3x3 smoothing, islands
+    dict(bR=7, bA=3, nGood=5, maxA=0.5, maxR=0.5, sR=4, sA=1, corrThresh=0.2, islandThresh=4, connectivity=4),
+])
+def test_cull_pipeline_matches_oracle(ctx, kw):
+    nA, nR = 150, 230
+    offR, offA, corr, mt = offsets_field(nA, nR, 7)
+    p = abi.CullParams(nR=nR, nA=nA, **kw)
+    g = ctx.cull(p, offR, offA, corr, mt)
+    o = oracle.cull(p, offR, offA, corr, mt)
+    _check(g, o)
+    assert g["nCulled"] == o["nCulled"]
+    if p.islandThresh > 0:
+        assert (g["nIslands"], g["nIslandPoints"]) == (o["nIslands"], o["nIslandPoints"])
+
+
+def test_cull_single_passes(ctx):
+    nA, nR = 80, 120
+    offR, offA, corr, mt = offsets_field(nA, nR, 8)
+    p = abi.CullParams(nR=nR, nA=nA)
+    g = ctx.cull(p, offR, offA, corr, mt, passes=("st",))
+    o = oracle.cull(p, offR, offA, corr, mt, passes=("st",))
+    assert _same(g["offR"], o["offR"]) and _same(g["offA"], o["offA"])
+    g = ctx.cull(p, offR, offA, corr, mt, passes=("st", "stats", "smooth", "islands"))
+    o = oracle.cull(p, offR, offA, corr, mt, passes=("st", "stats", "smooth", "islands"))
+    _check(g, o)
+
+
+def test_cull_mask_single_mt_and_sim(ctx):
+    nA, nR = 90, 140
+    offR, offA, corr, mt = offsets_field(nA, nR, 9)
+    rng = np.random.default_rng(3)
+    mask = rng.integers(0, 8, (nA, nR)).astype(np.uint8)
+    simR = (0.5 * rng.standard_normal((nA, nR))).astype(np.float32)
+    simA = (0.5 * rng.standard_normal((nA, nR))).astype(np.float32)
+    p = abi.CullParams(nR=nR, nA=nA, singleMT=2, useSim=1, islandThresh=6)
+    g = ctx.cull(p, offR, offA, corr, mt, mask=mask, simR=simR, simA=simA)
+    o = oracle.cull(p, offR, offA, corr, mt, mask=mask, simR=simR, simA=simA)
+    _check(g, o)
+
+
+def test_cull_large_grid_keep_mask(ctx):
+    """Keep masks on a 700 x 993 grid (rows of the large strack workload's grid)."""
+    nA, nR = 700, 993
+    offR, offA, corr, mt = offsets_field(nA, nR, 10)
+    p = abi.CullParams(nR=nR, nA=nA, bR=5, bA=5, nGood=12, sR=3, sA=3, islandThresh=10, nCullPasses=3)
+    g = ctx.cull(p, offR, offA, corr, mt)
+    t = ctx.timing()
+    o = oracle.cull(p, offR, offA, corr, mt)
+    _check(g, o)
+    print("cull 700x993:", t)
+    assert o["nIslands"] > 0
