@@ -56,6 +56,32 @@ def _compile(src, verbose):
     return obj
 
 
+HOST = os.path.join(HERE, "host")
+BINDIR = os.path.join(HERE, "bin")
+CC = os.environ.get("CC", "gcc")
+
+
+def build_cli():
+    """The drop-in command lines strack, strackw and cullst (C, linked to the library)."""
+    os.makedirs(BINDIR, exist_ok=True)
+    common = [os.path.join(HOST, "sbio.c")]
+    deps = glob.glob(os.path.join(HOST, "*.[ch]")) + [LIB, os.path.join(INCLUDE, "speckle_b200.h")]
+    link = ["-L" + LIBDIR, "-lspeckle_b200", "-Wl,-rpath,$ORIGIN/../lib", "-lm"]
+    tools = {"strack": (["track_main.c"], []), "strackw": (["track_main.c"], ["-DSTRACKW"]),
+             "cullst": (["cullst_main.c"], [])}
+    out = []
+    for name, (srcs, defs) in tools.items():
+        exe = os.path.join(BINDIR, name)
+        if _stale(exe, deps):
+            cmd = [CC, "-O2", "-std=gnu11", "-Wall", "-Wno-unused-result"] + defs + \
+                [os.path.join(HOST, s) for s in srcs] + common + ["-o", exe] + link
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"building {name} failed:\n{r.stderr}")
+        out.append(exe)
+    return out
+
+
 def build(verbose=False):
     os.makedirs(OBJ, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
@@ -67,6 +93,7 @@ def build(verbose=False):
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr}")
+    build_cli()
     return LIB
 
 
