@@ -177,27 +177,53 @@ struct RegDFT {
 // ---------------------------------------------------------------- line FFTs
 // Lines are addressed as base + (l % NLI) * LS + (l / NLI) * IS (NLI lines per
 // image, several images side by side).  Element k of a line is at k * ES.
-template <int N1, int N2, int DIR, int NL, int NLI, int NT>
-__device__ __forceinline__ void fft_lines(float2* base, int LS, int ES, int IS, const float2* __restrict__ tw)
+// All strides are compile-time constants, so addresses fold to immediates.
+//
+// Step 1 takes its inputs from `src(l, k)` and step 2 hands its outputs to
+// `dst(l, k1, k2, value)` (output index k = k1 + N1 * k2, k2 a compile-time
+// constant after unrolling); `base` holds the intermediate.  With the identity
+// functors the transform is in place.  src may gather from another buffer or
+// apply an element-wise map (in place is then still safe: step 1 of a thread
+// writes exactly the slots it read).  When src reads slots of `base` that other
+// threads write in step 1 (a permuting gather within the same buffer), set
+// SYNC1: every input is loaded before the first store.  dst is called after a
+// barrier that follows the last read of `base`, so it may overwrite `base`.
+template <int N1, int N2, int DIR, int NL, int NLI, int NT, int LS, int ES, int IS, bool SYNC1, typename Src,
+          typename Dst>
+__device__ __forceinline__ void fft_lines_io(float2* base, Src src, Dst dst, const float2* __restrict__ tw)
 {
     constexpr int N = N1 * N2;
     constexpr int T1 = NL * N2;
     constexpr int R1 = (T1 + NT - 1) / NT;
     const int tid = threadIdx.x;
+    float2 v[R1][N1];
+    auto step1 = [&](int r) {
+        const int t = tid + r * NT;
+        const int l = t % NL, n2 = t / NL;
+        float2* p = base + (l % NLI) * LS + (l / NLI) * IS + n2 * ES;
+        RegDFT<N1, DIR, N>::run(v[r], tw);
+        // k1 * n2 < N1 * N2 = N: the twiddle index needs no reduction
+#pragma unroll
+        for (int k1 = 1; k1 < N1; ++k1) v[r][k1] = twmul_rt<DIR>(v[r][k1], tw, k1 * n2);
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) p[(N2 * k1) * ES] = v[r][k1];
+    };
 #pragma unroll
     for (int r = 0; r < R1; ++r) {
         const int t = tid + r * NT;
         if (T1 % NT == 0 || t < T1) {
             const int l = t % NL, n2 = t / NL;
-            float2* p = base + (l % NLI) * LS + (l / NLI) * IS + n2 * ES;
-            float2 v[N1];
 #pragma unroll
-            for (int n1 = 0; n1 < N1; ++n1) v[n1] = p[(N2 * n1) * ES];
-            RegDFT<N1, DIR, N>::run(v, tw);
+            for (int n1 = 0; n1 < N1; ++n1) v[r][n1] = src(l, N2 * n1 + n2);
+            if constexpr (!SYNC1) step1(r);
+        }
+    }
+    if constexpr (SYNC1) {
+        __syncthreads();
 #pragma unroll
-            for (int k1 = 1; k1 < N1; ++k1) v[k1] = twmul_rt<DIR>(v[k1], tw, (k1 * n2) % N);
-#pragma unroll
-            for (int k1 = 0; k1 < N1; ++k1) p[(N2 * k1) * ES] = v[k1];
+        for (int r = 0; r < R1; ++r) {
+            const int t = tid + r * NT;
+            if (T1 % NT == 0 || t < T1) step1(r);
         }
     }
     __syncthreads();
@@ -221,12 +247,21 @@ __device__ __forceinline__ void fft_lines(float2* base, int LS, int ES, int IS, 
         const int t = tid + r * NT;
         if (T2 % NT == 0 || t < T2) {
             const int l = t % NL, k1 = t / NL;
-            float2* p = base + (l % NLI) * LS + (l / NLI) * IS + k1 * ES;
 #pragma unroll
-            for (int k2 = 0; k2 < N2; ++k2) p[(N1 * k2) * ES] = v2[r][k2];
+            for (int k2 = 0; k2 < N2; ++k2) dst(l, k1, k2, v2[r][k2]);
         }
     }
     __syncthreads();
+}
+
+// In-place transform of the lines (identity src/dst).
+template <int N1, int N2, int DIR, int NL, int NLI, int NT, int LS, int ES, int IS>
+__device__ __forceinline__ void fft_lines(float2* base, const float2* __restrict__ tw)
+{
+    auto at = [base](int l, int k) -> float2* { return base + (l % NLI) * LS + (l / NLI) * IS + k * ES; };
+    auto src = [at](int l, int k) { return *at(l, k); };
+    auto dst = [at](int l, int k1, int k2, float2 z) { *at(l, k1 + N1 * k2) = z; };
+    fft_lines_io<N1, N2, DIR, NL, NLI, NT, LS, ES, IS, false>(base, src, dst, tw);
 }
 
 // Factorisation used for each supported transform length.
@@ -249,12 +284,12 @@ template <> struct Split<512> { static constexpr int N1 = 32, N2 = 16; };
 
 // 2-D transform of NIMG row-major N x N images in shared memory (row stride
 // RS float2, image stride IS float2): rows (range) then columns (azimuth).
-template <int N, int DIR, int NIMG, int NT>
-__device__ __forceinline__ void fft2d_smem(float2* base, int RS, int IS, const float2* __restrict__ tw)
+template <int N, int DIR, int NIMG, int NT, int RS, int IS>
+__device__ __forceinline__ void fft2d_smem(float2* base, const float2* __restrict__ tw)
 {
     constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
-    fft_lines<N1, N2, DIR, N * NIMG, N, NT>(base, RS, 1, IS, tw);  // rows: line = row
-    fft_lines<N1, N2, DIR, N * NIMG, N, NT>(base, 1, RS, IS, tw);  // columns: line = column
+    fft_lines<N1, N2, DIR, N * NIMG, N, NT, RS, 1, IS>(base, tw);  // rows: line = row
+    fft_lines<N1, N2, DIR, N * NIMG, N, NT, 1, RS, IS>(base, tw);  // columns: line = column
 }
 
 // 2-D transform of an N x N row-major array anywhere in memory (row stride N;
@@ -272,7 +307,7 @@ __device__ __forceinline__ void fft2d_staged(float2* g, float2* tile, const floa
             tile[l * (N + 1) + k] = g[(size_t)(r0 + l) * N + k];
         }
         __syncthreads();
-        fft_lines<N1, N2, DIR, G, G, NT>(tile, N + 1, 1, 0, tw);
+        fft_lines<N1, N2, DIR, G, G, NT, N + 1, 1, 0>(tile, tw);
         for (int e = tid; e < G * N; e += NT) {
             const int l = e / N, k = e % N;
             g[(size_t)(r0 + l) * N + k] = tile[l * (N + 1) + k];
@@ -285,7 +320,7 @@ __device__ __forceinline__ void fft2d_staged(float2* g, float2* tile, const floa
             tile[k * (G + 1) + l] = g[(size_t)k * N + c0 + l];
         }
         __syncthreads();
-        fft_lines<N1, N2, DIR, G, G, NT>(tile, 1, G + 1, 0, tw);
+        fft_lines<N1, N2, DIR, G, G, NT, 1, G + 1, 0>(tile, tw);
         for (int e = tid; e < N * G; e += NT) {
             const int k = e / G, l = e % G;
             g[(size_t)k * N + c0 + l] = tile[k * (G + 1) + l];

@@ -22,22 +22,23 @@ namespace sbk {
 
 template <int W, int NT>
 struct CmplxSmem {
-    static constexpr int RS = W + 1;
-    static constexpr int IMG = W * RS;  // float2
-    static constexpr size_t bytes =
-        sizeof(float2) * (2 * IMG) + sizeof(float) * (2 * W * W) + sizeof(float2) * (W + W + OSW * NFAST) +
-        sizeof(float2) * (NFAST * OSW) + sizeof(float) * (NFAST * NFAST) + sizeof(double) * (NT / 32) * 8 +
-        sizeof(int) * (3 * (NT / 32) + 8) + 64;
+    static constexpr int RS = W + 1;    // odd row stride: row passes are bank-conflict free
+    static constexpr int IMG = W * RS;  // float2 per buffer; three buffers X, Y, Z
+    static constexpr size_t bytes = sizeof(float2) * (3 * IMG) + sizeof(float2) * (W + W + OSW * NFAST) +
+                                    sizeof(float2) * (NFAST * OSW) + sizeof(float) * (NFAST * NFAST) +
+                                    sizeof(double) * (NT / 32) * 8 + sizeof(int) * (3 * (NT / 32) + 8) + 64;
 };
 
-// |c| of the 2W x 2W surface at unshifted index (cy, cx).  The four parity
-// planes live at float offsets poff(q) from the start of shared memory:
-// planes 0, 1 in M, plane 2 over B, plane 3 over A.
+// |c| of the 2W x 2W surface at unshifted index (cy, cx).  The parity plane
+// (e1, e2) = (cy & 1, cx & 1) is a W x W float array at float offset poff(q),
+// q = 2 e1 + e2, from the start of shared memory (buffers X | Y | Z of 2W(W+1)
+// floats each): (0,0) X[0, W^2), (0,1) X[W^2, 2W^2), (1,0) the last W^2 floats
+// of Y, (1,1) Z[0, W^2).
 template <int W>
 __device__ __forceinline__ int poff(int q)
 {
-    constexpr int IMGF = 2 * W * (W + 1);  // one image region, in floats
-    return q == 3 ? 0 : (q == 2 ? IMGF : 2 * IMGF + (q & 1) * W * W);
+    constexpr int IMGF = 2 * W * (W + 1);
+    return q == 0 ? 0 : (q == 1 ? W * W : (q == 2 ? 2 * IMGF - W * W : 2 * IMGF));
 }
 template <int W>
 __device__ __forceinline__ float cmap(const float* sm, int cy, int cx)
@@ -53,24 +54,91 @@ __device__ __forceinline__ float fmap(const float* sm, int y, int x)
     return cmap<W>(sm, cy, cx);
 }
 
-template <int W, int NT>
+template <bool F32>
+__device__ __forceinline__ float2 load_sample_t(const void* __restrict__ img, int nr, int row, int col, int byteOrder)
+{
+    const size_t k = (size_t)row * (size_t)nr + (size_t)col;
+    if constexpr (F32) {
+        uint2 w = __ldg(reinterpret_cast<const uint2*>(img) + k);
+        if (byteOrder == SB_MSB) {
+            w.x = bswap32(w.x);
+            w.y = bswap32(w.y);
+        }
+        return make_float2(__uint_as_float(w.x) * 1000.f, __uint_as_float(w.y) * 1000.f);
+    } else {
+        uint32_t w = __ldg(reinterpret_cast<const uint32_t*>(img) + k);
+        if (byteOrder == SB_MSB) w = bswap16x2(w);
+        return make_float2((float)(int16_t)(w & 0xffffu), (float)(int16_t)(w >> 16));
+    }
+}
+
+// Final store of a column pass of the padded inverse for parity (E1, E2):
+// |c| goes to the parity plane and the thread's running findCPeak maximum is
+// updated.  The maximum is a 64-bit key (bits of |c|) << 32 | ~rank, so the
+// larger value wins and equal values go to the earlier position in findCPeak's
+// scan order (cpeak_rank); values that are not > 0 (zero, NaN) never win.  The
+// rank is folded from compile-time parts: the output row is
+// m1 = k1 + N1 k2, so cy = 2 m1 + E1 lies in the upper half (cy >= W) exactly
+// when k2 >= N2 / 2.
+template <int W, int N1, int N2, int E1, int E2>
+struct MagArgmax {
+    float* plane;
+    unsigned long long& best;
+    __device__ __forceinline__ void operator()(int l, int k1, int k2, float2 z) const
+    {
+        static_assert(N2 % 2 == 0, "the half test needs an even N2");
+        const float v = sqrtf(z.x * z.x + z.y * z.y);
+        plane[(k1 + N1 * k2) * W + l] = v;
+        const int cx = 2 * l + E2;
+        const bool xi = cx < W;  // fftshifted x >= W
+        const int j = xi ? cx : cx - W;
+        const bool yi = k2 < N2 / 2;  // fftshifted y >= W
+        const int i = 2 * k1 + E1 + 2 * N1 * k2 - (yi ? 0 : W);
+        const int q = (!yi && !xi) ? 0 : ((yi && xi) ? 1 : (yi ? 2 : 3));
+        const unsigned rank = (unsigned)((i * W + j) * 4 + q);
+        const unsigned vb = v > 0.f ? __float_as_uint(v) : 0u;
+        const unsigned long long key = ((unsigned long long)vb << 32) | (0xffffffffu - rank);
+        best = key > best ? key : best;
+    }
+};
+
+__device__ __forceinline__ unsigned long long block_max_u64(unsigned long long v, unsigned long long* scratch)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long u = __shfl_xor_sync(0xffffffffu, v, o);
+        v = u > v ? u : v;
+    }
+    if (lane == 0) scratch[warp] = v;
+    __syncthreads();
+    v = scratch[0];
+    for (int w = 1; w < nw; ++w) v = scratch[w] > v ? scratch[w] : v;
+    __syncthreads();
+    return v;
+}
+
+template <int W, int NT, bool F32>
 __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(CmplxArgs a)
 {
     using S = CmplxSmem<W, NT>;
     constexpr int RS = S::RS, IMG = S::IMG;
     constexpr int W2 = 2 * W;
+    constexpr int N1 = sbfft::Split<W>::N1, N2 = sbfft::Split<W>::N2;
+    static_assert(NT == 8 * W, "eight threads per column");
+    constexpr int RPT = W / 8;  // consecutive rows per thread in the load phase
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    float2* A = reinterpret_cast<float2*>(smem_raw);
-    float2* B = A + IMG;
-    float* M = reinterpret_cast<float*>(B + IMG);
-    float2* twW = reinterpret_cast<float2*>(M + 2 * W * W);
+    float2* X = reinterpret_cast<float2*>(smem_raw);
+    float2* Y = X + IMG;
+    float2* Z = Y + IMG;
+    float2* twW = Z + IMG;
     float2* tau = twW + W;
     float2* osA = tau + W;
     float2* T = osA + OSW * NFAST;
     float* blk = reinterpret_cast<float*>(T + NFAST * OSW);
     double* red = reinterpret_cast<double*>(blk + NFAST * NFAST);
     int* isc = reinterpret_cast<int*>(red + (NT / 32) * 8);
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x;
 
     for (int e = tid; e < W; e += NT) {
         twW[e] = a.twW[e];
@@ -80,25 +148,22 @@ __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(Cmp
     __syncthreads();
 
     float* smf = reinterpret_cast<float*>(smem_raw);
-    const bool isFloat = a.sampleType == SB_CFLOAT32;
-    const float thr = isFloat ? 1e-15f : 1e-9f;
+    const float thr = F32 ? 1e-15f : 1e-9f;
     const float thrAll = thr * W * W;
+    const int jc = tid % W, i0 = (tid / W) * RPT;  // load phase: column jc, rows i0 .. i0+RPT-1
 
     for (int it = blockIdx.x; it < a.nList; it += gridDim.x) {
         const int p = a.list[it];
         const PointPlan pl = a.plan[p];
         // ---------------------------------------------------- getPatches
         double s[7] = {0, 0, 0, 0, 0, 0, 0};
-        for (int e = tid; e < W * W; e += NT) {
-            const int i = e / W, j = e % W;
-            float2 z1 = load_sample(a.img1, a.nr1, pl.a1 + i, pl.r1 + j, a.sampleType, a.byteOrder);
-            float2 z2 = load_sample(a.img2, a.nr2, pl.a2 + i, pl.r2 + j, a.sampleType, a.byteOrder);
-            if (isFloat) {
-                z1.x *= 1000.f; z1.y *= 1000.f;
-                z2.x *= 1000.f; z2.y *= 1000.f;
-            }
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) {
+            const int i = i0 + r;
+            float2 z1 = load_sample_t<F32>(a.img1, a.nr1, pl.a1 + i, pl.r1 + jc, a.byteOrder);
+            float2 z2 = load_sample_t<F32>(a.img2, a.nr2, pl.a2 + i, pl.r2 + jc, a.byteOrder);
             if (a.hanning) {
-                const float h = a.hanning[e];
+                const float h = __ldg(a.hanning + i * W + jc);
                 z2.x *= h;
                 z2.y *= h;
             }
@@ -111,8 +176,8 @@ __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(Cmp
             s[3] += z1.y;
             s[4] += z2.x;
             s[5] += z2.y;
-            A[i * RS + j] = z1;
-            B[i * RS + j] = z2;
+            X[i * RS + jc] = z1;
+            Z[i * RS + jc] = z2;
         }
         block_allsum<7, NT>(s, red);
         const bool haveData = !(s[6] > 20.0) && !(s[0] < thrAll || s[1] < thrAll);
@@ -126,19 +191,30 @@ __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(Cmp
             continue;  // uniform across the block
         }
         // ---------------------------------------------------- Doppler (lag-1 sums)
+        // Each thread walks its own column run, the row below the run included.
         const double n = (double)(W * W);
         const double m1r = s[2] / n, m1i = s[3] / n, m2r = s[4] / n, m2i = s[5] / n;
         double d[4] = {0, 0, 0, 0};
-        for (int e = tid; e < (W - 1) * W; e += NT) {
-            const int i = e / W, j = e % W;
-            const float2 p0 = A[i * RS + j], p1 = A[(i + 1) * RS + j];
-            double ar = (double)p1.x - m1r, ai = (double)p1.y - m1i, br = (double)p0.x - m1r, bi = (double)p0.y - m1i;
-            d[0] += ar * br + ai * bi;
-            d[1] += ai * br - ar * bi;
-            const float2 q0 = B[i * RS + j], q1 = B[(i + 1) * RS + j];
-            ar = (double)q1.x - m2r; ai = (double)q1.y - m2i; br = (double)q0.x - m2r; bi = (double)q0.y - m2i;
-            d[2] += ar * br + ai * bi;
-            d[3] += ai * br - ar * bi;
+        {
+            float2 q1 = X[i0 * RS + jc], q2 = Z[i0 * RS + jc];
+            double br1 = (double)q1.x - m1r, bi1 = (double)q1.y - m1i;
+            double br2 = (double)q2.x - m2r, bi2 = (double)q2.y - m2i;
+            const int rEnd = i0 + RPT < W ? RPT : RPT - 1;
+#pragma unroll
+            for (int r = 1; r <= RPT; ++r) {
+                if (r <= rEnd) {
+                    q1 = X[(i0 + r) * RS + jc];
+                    q2 = Z[(i0 + r) * RS + jc];
+                    const double ar1 = (double)q1.x - m1r, ai1 = (double)q1.y - m1i;
+                    const double ar2 = (double)q2.x - m2r, ai2 = (double)q2.y - m2i;
+                    d[0] += ar1 * br1 + ai1 * bi1;
+                    d[1] += ai1 * br1 - ar1 * bi1;
+                    d[2] += ar2 * br2 + ai2 * bi2;
+                    d[3] += ai2 * br2 - ar2 * bi2;
+                    br1 = ar1; bi1 = ai1;
+                    br2 = ar2; bi2 = ai2;
+                }
+            }
         }
         block_allsum<4, NT>(d, red);
         const int azShift = dop_shift(d[0], d[1], d[2], d[3], W, W);
@@ -160,99 +236,64 @@ __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(Cmp
                 ph *= ptod;
                 double sn, cs;
                 sincos(ph, &sn, &cs);
-                const float2 z = A[i * RS + j];
-                A[i * RS + j] = make_float2((float)(z.x * cs - z.y * sn), (float)(z.x * sn + z.y * cs));
+                const float2 z = X[i * RS + j];
+                X[i * RS + j] = make_float2((float)(z.x * cs - z.y * sn), (float)(z.x * sn + z.y * cs));
             }
             __syncthreads();
         }
-        // ---------------------------------------------------- spectra, cross spectrum
-        sbfft::fft2d_smem<W, -1, 2, NT>(A, RS, IMG, twW);
-        for (int e = tid; e < W * W; e += NT) {
-            const int i = e / W, j = e % W;
-            A[i * RS + j] = sbfft::cconjmul(A[i * RS + j], B[i * RS + j]);
+        // ---------------------------------------------------- spectra of both patches (X and Z)
+        sbfft::fft2d_smem<W, -1, 2, NT, RS, 2 * IMG>(X, twW);
+        // ---------------------------------------------------- padded inverse
+        // Row passes (over k2) for e2 = 0, 1 read the cross spectrum
+        // X conj(Z) with the Doppler row shift folded in; the per-row factor
+        // tau_e1[k1] commutes with them and is applied in the column passes,
+        // so two row passes serve the four parities.
+        auto rowOf = [azShift](int l) {
+            const int r = l + azShift;
+            return r >= W ? r - W : r;
+        };
+        auto rowId = [](float2* b) {
+            return [b](int l, int k1, int k2, float2 z) { b[l * RS + k1 + N1 * k2] = z; };
+        };
+        {
+            auto src0 = [=](int l, int k) {
+                const int o = rowOf(l) * RS + k;
+                return sbfft::cconjmul(X[o], Z[o]);
+            };
+            sbfft::fft_lines_io<N1, N2, 1, W, W, NT, RS, 1, 0, false>(Y, src0, rowId(Y), twW);
+            auto src1 = [=](int l, int k) {
+                const int o = rowOf(l) * RS + k;
+                return sbfft::cmul(sbfft::cconjmul(X[o], Z[o]), tau[k]);
+            };
+            sbfft::fft_lines_io<N1, N2, 1, W, W, NT, RS, 1, 0, true>(Z, src1, rowId(Z), twW);
         }
-        __syncthreads();
-        // ---------------------------------------------------- padded inverse, four parities
-        constexpr int EPT = (W * W + NT - 1) / NT;
-#pragma unroll 1
-        for (int par = 0; par < 4; ++par) {
-            const int e1 = par >> 1, e2 = par & 1;
-            float2* dst = par < 3 ? B : A;
-            if (par < 3) {
-                for (int e = tid; e < W * W; e += NT) {
-                    const int k1 = e / W, k2 = e % W;
-                    float2 v = A[((k1 + azShift) % W) * RS + k2];
-                    if (e1) v = sbfft::cmul(v, tau[k1]);
-                    if (e2) v = sbfft::cmul(v, tau[k2]);
-                    dst[k1 * RS + k2] = v;
-                }
-            } else {
-                float2 hold[EPT];
-#pragma unroll
-                for (int r = 0; r < EPT; ++r) {
-                    const int e = tid + r * NT;
-                    if (e < W * W) {
-                        const int k1 = e / W, k2 = e % W;
-                        float2 v = A[((k1 + azShift) % W) * RS + k2];
-                        v = sbfft::cmul(v, tau[k1]);
-                        v = sbfft::cmul(v, tau[k2]);
-                        hold[r] = v;
-                    }
-                }
-                __syncthreads();
-#pragma unroll
-                for (int r = 0; r < EPT; ++r) {
-                    const int e = tid + r * NT;
-                    if (e < W * W) dst[(e / W) * RS + (e % W)] = hold[r];
-                }
-            }
-            __syncthreads();
-            sbfft::fft2d_smem<W, 1, 1, NT>(dst, RS, 0, twW);
-            float* plane = smf + poff<W>(par);
-            if (par < 2) {
-                for (int e = tid; e < W * W; e += NT) {
-                    const float2 z = dst[(e / W) * RS + (e % W)];
-                    plane[e] = sqrtf(z.x * z.x + z.y * z.y);
-                }
-            } else {
-                float hv[EPT];
-#pragma unroll
-                for (int r = 0; r < EPT; ++r) {
-                    const int e = tid + r * NT;
-                    if (e < W * W) {
-                        const float2 z = dst[(e / W) * RS + (e % W)];
-                        hv[r] = sqrtf(z.x * z.x + z.y * z.y);
-                    }
-                }
-                __syncthreads();
-#pragma unroll
-                for (int r = 0; r < EPT; ++r) {
-                    const int e = tid + r * NT;
-                    if (e < W * W) plane[e] = hv[r];
-                }
-            }
-            __syncthreads();
+        // Column passes (over k1): R0 = Y, R1 = Z.  Each ends in |c| and the
+        // running argmax; buffers are placed so no pass overwrites an input
+        // still needed or a finished plane.
+        unsigned long long best = 0ull;
+        {
+            auto colOf = [](const float2* b) { return [b](int l, int k) { return b[k * RS + l]; }; };
+            auto colTau = [=](const float2* b) {
+                return [b, tau](int l, int k) { return sbfft::cmul(b[k * RS + l], tau[k]); };
+            };
+            float2* D = X + (W * W) / 2;  // spans the end of X and the start of Y
+            sbfft::fft_lines_io<N1, N2, 1, W, W, NT, 1, RS, 0, false>(
+                X, colOf(Y), MagArgmax<W, N1, N2, 0, 0>{smf + poff<W>(0), best}, twW);
+            sbfft::fft_lines_io<N1, N2, 1, W, W, NT, 1, RS, 0, false>(
+                Y, colTau(Y), MagArgmax<W, N1, N2, 1, 0>{smf + poff<W>(2), best}, twW);
+            sbfft::fft_lines_io<N1, N2, 1, W, W, NT, 1, RS, 0, false>(
+                D, colOf(Z), MagArgmax<W, N1, N2, 0, 1>{smf + poff<W>(1), best}, twW);
+            sbfft::fft_lines_io<N1, N2, 1, W, W, NT, 1, RS, 0, false>(
+                Z, colTau(Z), MagArgmax<W, N1, N2, 1, 1>{smf + poff<W>(3), best}, twW);
         }
         // ---------------------------------------------------- findCPeak
-        ArgMax best;
-        best.v = 0.f;
-        best.rank = 0x7fffffff;
-        best.pos = 0;
-        for (int e = tid; e < W2 * W2; e += NT) {
-            const int y = e / W2, x = e % W2;
-            const float v = fmap<W>(smf, y, x);
-            const int rk = cpeak_rank(y, x, W);
-            if (v > 0.f && am_better(v, rk, best.v, best.rank)) {
-                best.v = v;
-                best.rank = rk;
-                best.pos = e;
-            }
-        }
-        best = block_argmax<NT>(best, isc);
+        best = block_max_u64(best, reinterpret_cast<unsigned long long*>(red));
         int iMax = 0, jMax = 0;
-        if (best.rank != 0x7fffffff) {
-            iMax = best.pos / W2;
-            jMax = best.pos % W2;
+        if ((best >> 32) != 0ull) {
+            const unsigned rank = 0xffffffffu - (unsigned)(best & 0xffffffffull);
+            const int q = rank & 3, ij = rank >> 2;
+            iMax = ij / W + ((q == 1 || q == 2) ? W : 0);
+            jMax = ij % W + ((q == 1 || q == 3) ? W : 0);
         }
         double cMax;
         const bool rejected = (iMax < (NFAST / 2) || iMax > (W2 - NFAST / 2) || jMax < (NFAST / 2) ||
@@ -306,15 +347,22 @@ __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(Cmp
     }
 }
 
+template <int W, int NT, bool F32>
+static cudaError_t launch_cmplx_t(const CmplxArgs& a, int nCta, cudaStream_t st)
+{
+    const size_t sm = CmplxSmem<W, NT>::bytes;
+    cudaError_t e = cudaFuncSetAttribute(strack_cmplx_kernel<W, NT, F32>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    strack_cmplx_kernel<W, NT, F32><<<nCta, NT, sm, st>>>(a);
+    return cudaGetLastError();
+}
+
 template <int W, int NT>
 static cudaError_t launch_cmplx(const CmplxArgs& a, int nCta, cudaStream_t st)
 {
-    const size_t sm = CmplxSmem<W, NT>::bytes;
-    cudaError_t e = cudaFuncSetAttribute(strack_cmplx_kernel<W, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)sm);
-    if (e != cudaSuccess) return e;
-    strack_cmplx_kernel<W, NT><<<nCta, NT, sm, st>>>(a);
-    return cudaGetLastError();
+    return a.sampleType == SB_CFLOAT32 ? launch_cmplx_t<W, NT, true>(a, nCta, st)
+                                       : launch_cmplx_t<W, NT, false>(a, nCta, st);
 }
 
 template <int W, int NT>
@@ -322,8 +370,8 @@ static int occupancy_cmplx()
 {
     int nb = 0;
     const size_t sm = CmplxSmem<W, NT>::bytes;
-    cudaFuncSetAttribute(strack_cmplx_kernel<W, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, strack_cmplx_kernel<W, NT>, NT, sm);
+    cudaFuncSetAttribute(strack_cmplx_kernel<W, NT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, strack_cmplx_kernel<W, NT, true>, NT, sm);
     return nb;
 }
 
