@@ -190,6 +190,26 @@ const float2* osA_table(sb_context* c)
     return (const float2*)sb_table(c, "osA", h);
 }
 
+// Real form of the oversampling matrix: A[n][t] = p(n) exp(+i pi t/8) D[n][t]
+// with |p(n)| = 1 and D[n][t] = 2 sum_{g=1/2..7/2} cos(2 pi g (n + 24 - 12 t)/96);
+// stored as the 48 x 8 floats of D followed by the 16 phases exp(i pi s/8).
+const float2* osD_table(sb_context* c)
+{
+    std::vector<float2> h(OSW * NFAST / 2 + 16);
+    float* f = reinterpret_cast<float*>(h.data());
+    for (int n = 0; n < OSW; ++n)
+        for (int t = 0; t < NFAST; ++t) {
+            const int d = (n + 24) - NOVER * t;
+            double v = 0.0;
+            for (int g2 = 1; g2 < NFAST; g2 += 2)  // g = g2 / 2
+                v += 2.0 * cos(kPi * (double)g2 * (double)d / (double)(NFAST * NOVER));
+            f[n * NFAST + t] = (float)v;
+        }
+    for (int s = 0; s < 16; ++s)
+        h[OSW * NFAST / 2 + s] = make_float2((float)cos(kPi * s / 8.0), (float)sin(kPi * s / 8.0));
+    return (const float2*)sb_table(c, "osD", h);
+}
+
 // computeHanning (speckleTrack.c:1830-1852), W x W, square windows.
 const float* hanning_table(sb_context* c, int W)
 {
@@ -527,6 +547,7 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
         a.twW = tw_table(c, W);
         a.tau = tau_table(c, W);
         a.osA = osA_table(c);
+        a.osD = osD_table(c);
         a.azThresh = p->azDefocusThresh;
         a.checkAzFocus = p->checkAzFocus;
         a.noComplex = p->noComplex;
@@ -538,7 +559,7 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
         }
         a.rec = drec;
         a.fit = dfit;
-        if (!a.twW || !a.tau || !a.osA || (p->hanningFlag && !a.hanning))
+        if (!a.twW || !a.tau || !a.osA || !a.osD || (p->hanningFlag && !a.hanning))
             return sb_ctx_fail(c, SB_ERR_NOMEM, "table allocation failed");
         int bpsm = cmplx_blocks_per_sm(W);
         if (bpsm <= 0) return sb_ctx_fail(c, SB_ERR_CUDA, "complex kernel cannot be resident (W=%d)", W);

@@ -175,6 +175,41 @@ struct RegDFT {
 };
 
 // ---------------------------------------------------------------- line FFTs
+// Step 2 of the line transforms (see fft_lines_io): radix-N2 DFTs over the N2
+// contiguous slots of every (line, k1), all loaded before the first store;
+// outputs go to dst(l, k1, k2, value).  Ends with a barrier.
+template <int N1, int N2, int DIR, int NL, int NLI, int NT, int LS, int ES, int IS, typename Dst>
+__device__ __forceinline__ void fft_step2(float2* base, Dst dst, const float2* __restrict__ tw)
+{
+    constexpr int N = N1 * N2;
+    constexpr int T2 = NL * N1;
+    constexpr int R2 = (T2 + NT - 1) / NT;
+    const int tid = threadIdx.x;
+    float2 v2[R2][N2];
+#pragma unroll
+    for (int r = 0; r < R2; ++r) {
+        const int t = tid + r * NT;
+        if (T2 % NT == 0 || t < T2) {
+            const int l = t % NL, k1 = t / NL;
+            const float2* p = base + (l % NLI) * LS + (l / NLI) * IS + (N2 * k1) * ES;
+#pragma unroll
+            for (int n2 = 0; n2 < N2; ++n2) v2[r][n2] = p[n2 * ES];
+            RegDFT<N2, DIR, N>::run(v2[r], tw);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < R2; ++r) {
+        const int t = tid + r * NT;
+        if (T2 % NT == 0 || t < T2) {
+            const int l = t % NL, k1 = t / NL;
+#pragma unroll
+            for (int k2 = 0; k2 < N2; ++k2) dst(l, k1, k2, v2[r][k2]);
+        }
+    }
+    __syncthreads();
+}
+
 // Lines are addressed as base + (l % NLI) * LS + (l / NLI) * IS (NLI lines per
 // image, several images side by side).  Element k of a line is at k * ES.
 // All strides are compile-time constants, so addresses fold to immediates.
@@ -227,31 +262,7 @@ __device__ __forceinline__ void fft_lines_io(float2* base, Src src, Dst dst, con
         }
     }
     __syncthreads();
-    constexpr int T2 = NL * N1;
-    constexpr int R2 = (T2 + NT - 1) / NT;
-    float2 v2[R2][N2];
-#pragma unroll
-    for (int r = 0; r < R2; ++r) {
-        const int t = tid + r * NT;
-        if (T2 % NT == 0 || t < T2) {
-            const int l = t % NL, k1 = t / NL;
-            const float2* p = base + (l % NLI) * LS + (l / NLI) * IS + (N2 * k1) * ES;
-#pragma unroll
-            for (int n2 = 0; n2 < N2; ++n2) v2[r][n2] = p[n2 * ES];
-            RegDFT<N2, DIR, N>::run(v2[r], tw);
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < R2; ++r) {
-        const int t = tid + r * NT;
-        if (T2 % NT == 0 || t < T2) {
-            const int l = t % NL, k1 = t / NL;
-#pragma unroll
-            for (int k2 = 0; k2 < N2; ++k2) dst(l, k1, k2, v2[r][k2]);
-        }
-    }
-    __syncthreads();
+    fft_step2<N1, N2, DIR, NL, NLI, NT, LS, ES, IS>(base, dst, tw);
 }
 
 // In-place transform of the lines (identity src/dst).
@@ -262,6 +273,67 @@ __device__ __forceinline__ void fft_lines(float2* base, const float2* __restrict
     auto src = [at](int l, int k) { return *at(l, k); };
     auto dst = [at](int l, int k1, int k2, float2 z) { *at(l, k1 + N1 * k2) = z; };
     fft_lines_io<N1, N2, DIR, NL, NLI, NT, LS, ES, IS, false>(base, src, dst, tw);
+}
+
+// Two transforms of the same NL input lines in one pass: with u = src(l, k),
+// the lines at base get DFT(u) and the lines at base + IS get
+// DFT(u * mul(l, k)).  Each input is read once; step 2 then runs over all
+// 2 NL lines (dst sees l in [0, 2 NL): l / NL selects the transform).
+// SYNC1 as in fft_lines_io.
+template <int N1, int N2, int DIR, int NL, int NT, int LS, int ES, int IS, bool SYNC1, typename Src, typename Mul,
+          typename Dst>
+__device__ __forceinline__ void fft_lines_dual(float2* base, Src src, Mul mul, Dst dst,
+                                               const float2* __restrict__ tw)
+{
+    constexpr int N = N1 * N2;
+    constexpr int T1 = NL * N2;
+    constexpr int R1 = (T1 + NT - 1) / NT;
+    const int tid = threadIdx.x;
+    float2 va[R1][N1], vb[R1][N1];
+    auto step1 = [&](int r) {
+        const int t = tid + r * NT;
+        const int l = t % NL, n2 = t / NL;
+        RegDFT<N1, DIR, N>::run(va[r], tw);
+        RegDFT<N1, DIR, N>::run(vb[r], tw);
+        float2* pa = base + l * LS + n2 * ES;
+        float2* pb = pa + IS;
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) {
+            if (k1 > 0) {
+                float2 w = tw[k1 * n2];
+                if (DIR > 0) w.y = -w.y;
+                va[r][k1] = cmul(va[r][k1], w);
+                vb[r][k1] = cmul(vb[r][k1], w);
+            }
+            pa[(N2 * k1) * ES] = va[r][k1];
+            pb[(N2 * k1) * ES] = vb[r][k1];
+        }
+    };
+#pragma unroll
+    for (int r = 0; r < R1; ++r) {
+        const int t = tid + r * NT;
+        if (T1 % NT == 0 || t < T1) {
+            const int l = t % NL, n2 = t / NL;
+#pragma unroll
+            for (int n1 = 0; n1 < N1; ++n1) {
+                const int k = N2 * n1 + n2;
+                const float2 u = src(l, k);
+                va[r][n1] = u;
+                vb[r][n1] = cmul(u, mul(l, k));
+            }
+            if constexpr (!SYNC1) step1(r);
+        }
+    }
+    if constexpr (SYNC1) {
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < R1; ++r) {
+            const int t = tid + r * NT;
+            if (T1 % NT == 0 || t < T1) step1(r);
+        }
+    }
+    __syncthreads();
+    fft_step2<N1, N2, DIR, 2 * NL, NL, NT, LS, ES, IS>(base, dst, tw);
 }
 
 // Factorisation used for each supported transform length.

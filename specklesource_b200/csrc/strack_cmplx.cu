@@ -24,9 +24,9 @@ template <int W, int NT>
 struct CmplxSmem {
     static constexpr int RS = W + 1;    // odd row stride: row passes are bank-conflict free
     static constexpr int IMG = W * RS;  // float2 per buffer; three buffers X, Y, Z
-    static constexpr size_t bytes = sizeof(float2) * (3 * IMG) + sizeof(float2) * (W + W + OSW * NFAST) +
-                                    sizeof(float2) * (NFAST * OSW) + sizeof(float) * (NFAST * NFAST) +
-                                    sizeof(double) * (NT / 32) * 8 + sizeof(int) * (3 * (NT / 32) + 8) + 64;
+    static constexpr int OSD = OSW * NFAST / 2 + 16;  // float2 of the real oversampling table
+    static constexpr size_t bytes = sizeof(float2) * (3 * IMG + 2 * W + OSD + NFAST * NFAST + NFAST * OSW) +
+                                    sizeof(float) * (NFAST * NFAST) + sizeof(double) * (NT / 32) * 8 + 64;
 };
 
 // |c| of the 2W x 2W surface at unshifted index (cy, cx).  The parity plane
@@ -72,51 +72,35 @@ __device__ __forceinline__ float2 load_sample_t(const void* __restrict__ img, in
     }
 }
 
-// Final store of a column pass of the padded inverse for parity (E1, E2):
+// Final store of a pair of column passes of the padded inverse, parities
+// (0, E2) and (1, E2) (line l < W: e1 = 0, else e1 = 1, column l mod W):
 // |c| goes to the parity plane and the thread's running findCPeak maximum is
-// updated.  The maximum is a 64-bit key (bits of |c|) << 32 | ~rank, so the
-// larger value wins and equal values go to the earlier position in findCPeak's
-// scan order (cpeak_rank); values that are not > 0 (zero, NaN) never win.  The
-// rank is folded from compile-time parts: the output row is
-// m1 = k1 + N1 k2, so cy = 2 m1 + E1 lies in the upper half (cy >= W) exactly
-// when k2 >= N2 / 2.
-template <int W, int N1, int N2, int E1, int E2>
+// updated.  The maximum is the am_key of |c| and its position in findCPeak's
+// scan order (cpeak_rank).  The rank is folded from compile-time parts: the
+// output row is m1 = k1 + N1 k2, so cy = 2 m1 + e1 lies in the upper half
+// (cy >= W) exactly when k2 >= N2 / 2.
+template <int W, int N1, int N2, int E2>
 struct MagArgmax {
-    float* plane;
+    float* plane0;  // parity (0, E2)
+    float* plane1;  // parity (1, E2)
     unsigned long long& best;
     __device__ __forceinline__ void operator()(int l, int k1, int k2, float2 z) const
     {
         static_assert(N2 % 2 == 0, "the half test needs an even N2");
+        const int e1 = l >= W;
+        const int col = l - (e1 ? W : 0);
         const float v = sqrtf(z.x * z.x + z.y * z.y);
-        plane[(k1 + N1 * k2) * W + l] = v;
-        const int cx = 2 * l + E2;
+        (e1 ? plane1 : plane0)[(k1 + N1 * k2) * W + col] = v;
+        const int cx = 2 * col + E2;
         const bool xi = cx < W;  // fftshifted x >= W
         const int j = xi ? cx : cx - W;
         const bool yi = k2 < N2 / 2;  // fftshifted y >= W
-        const int i = 2 * k1 + E1 + 2 * N1 * k2 - (yi ? 0 : W);
+        const int i = 2 * k1 + e1 + 2 * N1 * k2 - (yi ? 0 : W);
         const int q = (!yi && !xi) ? 0 : ((yi && xi) ? 1 : (yi ? 2 : 3));
-        const unsigned rank = (unsigned)((i * W + j) * 4 + q);
-        const unsigned vb = v > 0.f ? __float_as_uint(v) : 0u;
-        const unsigned long long key = ((unsigned long long)vb << 32) | (0xffffffffu - rank);
+        const unsigned long long key = am_key(v, (unsigned)((i * W + j) * 4 + q));
         best = key > best ? key : best;
     }
 };
-
-__device__ __forceinline__ unsigned long long block_max_u64(unsigned long long v, unsigned long long* scratch)
-{
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        const unsigned long long u = __shfl_xor_sync(0xffffffffu, v, o);
-        v = u > v ? u : v;
-    }
-    if (lane == 0) scratch[warp] = v;
-    __syncthreads();
-    v = scratch[0];
-    for (int w = 1; w < nw; ++w) v = scratch[w] > v ? scratch[w] : v;
-    __syncthreads();
-    return v;
-}
 
 template <int W, int NT, bool F32>
 __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(CmplxArgs a)
@@ -133,18 +117,19 @@ __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(Cmp
     float2* Z = Y + IMG;
     float2* twW = Z + IMG;
     float2* tau = twW + W;
-    float2* osA = tau + W;
-    float2* T = osA + OSW * NFAST;
+    float2* osD2 = tau + W;  // 16-byte aligned: every region before it is a multiple of 16 bytes
+    float2* Yb = osD2 + S::OSD;
+    float2* T = Yb + NFAST * NFAST;
     float* blk = reinterpret_cast<float*>(T + NFAST * OSW);
     double* red = reinterpret_cast<double*>(blk + NFAST * NFAST);
-    int* isc = reinterpret_cast<int*>(red + (NT / 32) * 8);
+    const float* osD = reinterpret_cast<const float*>(osD2);
     const int tid = threadIdx.x;
 
     for (int e = tid; e < W; e += NT) {
         twW[e] = a.twW[e];
         tau[e] = a.tau[e];
     }
-    for (int e = tid; e < OSW * NFAST; e += NT) osA[e] = a.osA[e];
+    for (int e = tid; e < S::OSD; e += NT) osD2[e] = a.osD[e];
     __syncthreads();
 
     float* smf = reinterpret_cast<float*>(smem_raw);
@@ -156,7 +141,9 @@ __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(Cmp
         const int p = a.list[it];
         const PointPlan pl = a.plan[p];
         // ---------------------------------------------------- getPatches
-        double s[7] = {0, 0, 0, 0, 0, 0, 0};
+        // per-thread partial sums over the RPT rows in float, block totals in double
+        float f[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        int nLow = 0;
 #pragma unroll
         for (int r = 0; r < RPT; ++r) {
             const int i = i0 + r;
@@ -169,16 +156,17 @@ __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(Cmp
             }
             const float pw1 = __fadd_rn(__fmul_rn(z1.x, z1.x), __fmul_rn(z1.y, z1.y));
             const float pw2 = __fadd_rn(__fmul_rn(z2.x, z2.x), __fmul_rn(z2.y, z2.y));
-            if (pw1 < thr || pw2 < thr) s[6] += 1.0;
-            s[0] += pw1;
-            s[1] += pw2;
-            s[2] += z1.x;
-            s[3] += z1.y;
-            s[4] += z2.x;
-            s[5] += z2.y;
+            nLow += (pw1 < thr || pw2 < thr);
+            f[0] += pw1;
+            f[1] += pw2;
+            f[2] += z1.x;
+            f[3] += z1.y;
+            f[4] += z2.x;
+            f[5] += z2.y;
             X[i * RS + jc] = z1;
             Z[i * RS + jc] = z2;
         }
+        double s[7] = {f[0], f[1], f[2], f[3], f[4], f[5], (double)nLow};
         block_allsum<7, NT>(s, red);
         const bool haveData = !(s[6] > 20.0) && !(s[0] < thrAll || s[1] < thrAll);
         if (!haveData) {
@@ -244,47 +232,38 @@ __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(Cmp
         // ---------------------------------------------------- spectra of both patches (X and Z)
         sbfft::fft2d_smem<W, -1, 2, NT, RS, 2 * IMG>(X, twW);
         // ---------------------------------------------------- padded inverse
-        // Row passes (over k2) for e2 = 0, 1 read the cross spectrum
-        // X conj(Z) with the Doppler row shift folded in; the per-row factor
-        // tau_e1[k1] commutes with them and is applied in the column passes,
-        // so two row passes serve the four parities.
-        auto rowOf = [azShift](int l) {
-            const int r = l + azShift;
-            return r >= W ? r - W : r;
-        };
-        auto rowId = [](float2* b) {
-            return [b](int l, int k1, int k2, float2 z) { b[l * RS + k1 + N1 * k2] = z; };
-        };
+        // One dual row pass (over k2) makes R0 (e2 = 0, into Y) and R1 (e2 = 1,
+        // times tau[k2], into Z) from the cross spectrum X conj(Z) with the
+        // Doppler row shift folded in.  The per-row factor tau_e1[k1] commutes
+        // with the row transform and is applied in the column passes, so two
+        // row transforms serve the four parities.
         {
-            auto src0 = [=](int l, int k) {
-                const int o = rowOf(l) * RS + k;
+            const int sh = azShift;
+            auto srcS = [X, Z, sh](int l, int k) {
+                const int r = l + sh;
+                const int o = (r >= W ? r - W : r) * RS + k;
                 return sbfft::cconjmul(X[o], Z[o]);
             };
-            sbfft::fft_lines_io<N1, N2, 1, W, W, NT, RS, 1, 0, false>(Y, src0, rowId(Y), twW);
-            auto src1 = [=](int l, int k) {
-                const int o = rowOf(l) * RS + k;
-                return sbfft::cmul(sbfft::cconjmul(X[o], Z[o]), tau[k]);
+            auto mulTau = [tau](int, int k) { return tau[k]; };
+            auto rowStore = [Y](int l, int k1, int k2, float2 z) {
+                Y[(l % W) * RS + (l / W) * IMG + k1 + N1 * k2] = z;
             };
-            sbfft::fft_lines_io<N1, N2, 1, W, W, NT, RS, 1, 0, true>(Z, src1, rowId(Z), twW);
+            sbfft::fft_lines_dual<N1, N2, 1, W, NT, RS, 1, IMG, true>(Y, srcS, mulTau, rowStore, twW);
         }
-        // Column passes (over k1): R0 = Y, R1 = Z.  Each ends in |c| and the
-        // running argmax; buffers are placed so no pass overwrites an input
-        // still needed or a finished plane.
+        // Dual column passes (over k1): R0 (Y) -> parities (0,0) into X and
+        // (1,0) in place; R1 (Z) -> (0,1) into D and (1,1) in place.  Each ends
+        // in |c| and the running argmax; the buffers are placed so that no pass
+        // overwrites an input still needed or a finished plane.
         unsigned long long best = 0ull;
         {
-            auto colOf = [](const float2* b) { return [b](int l, int k) { return b[k * RS + l]; }; };
-            auto colTau = [=](const float2* b) {
-                return [b, tau](int l, int k) { return sbfft::cmul(b[k * RS + l], tau[k]); };
-            };
+            auto mulTau = [tau](int, int k) { return tau[k]; };
+            auto colY = [Y](int l, int k) { return Y[k * RS + l]; };
+            sbfft::fft_lines_dual<N1, N2, 1, W, NT, 1, RS, IMG, false>(
+                X, colY, mulTau, MagArgmax<W, N1, N2, 0>{smf + poff<W>(0), smf + poff<W>(2), best}, twW);
             float2* D = X + (W * W) / 2;  // spans the end of X and the start of Y
-            sbfft::fft_lines_io<N1, N2, 1, W, W, NT, 1, RS, 0, false>(
-                X, colOf(Y), MagArgmax<W, N1, N2, 0, 0>{smf + poff<W>(0), best}, twW);
-            sbfft::fft_lines_io<N1, N2, 1, W, W, NT, 1, RS, 0, false>(
-                Y, colTau(Y), MagArgmax<W, N1, N2, 1, 0>{smf + poff<W>(2), best}, twW);
-            sbfft::fft_lines_io<N1, N2, 1, W, W, NT, 1, RS, 0, false>(
-                D, colOf(Z), MagArgmax<W, N1, N2, 0, 1>{smf + poff<W>(1), best}, twW);
-            sbfft::fft_lines_io<N1, N2, 1, W, W, NT, 1, RS, 0, false>(
-                Z, colTau(Z), MagArgmax<W, N1, N2, 1, 1>{smf + poff<W>(3), best}, twW);
+            auto colZ = [Z](int l, int k) { return Z[k * RS + l]; };
+            sbfft::fft_lines_dual<N1, N2, 1, W, NT, 1, RS, 2 * IMG - (W * W) / 2, false>(
+                D, colZ, mulTau, MagArgmax<W, N1, N2, 1>{smf + poff<W>(1), smf + poff<W>(3), best}, twW);
         }
         // ---------------------------------------------------- findCPeak
         best = block_max_u64(best, reinterpret_cast<unsigned long long*>(red));
@@ -310,7 +289,7 @@ __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(Cmp
                 blk[tid] = fmap<W>(smf, iMax - NFAST / 2 + t1, jMax - NFAST / 2 + t2);
             }
             __syncthreads();
-            const ArgMax ob = oversample_peak<NT>(blk, osA, T, isc);
+            const ArgMax ob = oversample_peak_real<NT>(blk, osD, Yb, T, reinterpret_cast<unsigned long long*>(red));
             const int iMax1 = ob.pos / OSW + (NFAST * NOVER) / 2 - 2 * NOVER;
             const int jMax1 = ob.pos % OSW + (NFAST * NOVER) / 2 - 2 * NOVER;
             cMax = (double)ob.v / (NFAST * NFAST);

@@ -22,6 +22,7 @@ struct CmplxArgs {
     const float2* twW;     // W_W^e forward twiddles, W entries
     const float2* tau;     // parity twiddles, W entries
     const float2* osA;     // 48 x 8 oversampling matrix
+    const float2* osD;     // real form of it: 48 x 8 floats D, then 16 phases
     float azThresh;
     int checkAzFocus, noComplex;
     int baseOn;
