@@ -91,8 +91,14 @@ extern "C" int sb_context_create(int device, sb_context** out)
         delete c;
         return SB_ERR_CUDA;
     }
+    if (cudaStreamCreateWithFlags(&c->copyStream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaStreamDestroy(c->stream);
+        delete c;
+        return SB_ERR_CUDA;
+    }
     for (int k = 0; k < 4; ++k) cudaEventCreate(&c->ev[k]);
     for (int k = 0; k < 16; ++k) cudaEventCreate(&c->sev[k]);
+    for (int k = 0; k < SB_MAX_BANDS; ++k) cudaEventCreateWithFlags(&c->chunkEv[k], cudaEventDisableTiming);
     *out = c;
     return SB_OK;
 }
@@ -102,12 +108,15 @@ extern "C" void sb_context_destroy(sb_context* c)
     if (!c) return;
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
+    cudaStreamSynchronize(c->copyStream);
     for (auto& kv : c->bufs)
         if (kv.second.ptr) cudaFree(kv.second.ptr);
     for (auto& kv : c->tables)
         if (kv.second) cudaFree(kv.second);
     for (int k = 0; k < 4; ++k) cudaEventDestroy(c->ev[k]);
     for (int k = 0; k < 16; ++k) cudaEventDestroy(c->sev[k]);
+    for (int k = 0; k < SB_MAX_BANDS; ++k) cudaEventDestroy(c->chunkEv[k]);
+    cudaStreamDestroy(c->copyStream);
     cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -373,6 +382,60 @@ int sb_image_to_device(sb_context* c, const sb_image* im, const char* name, cons
     return SB_OK;
 }
 
+// Banded upload for sb_strack: host images go up in nb azimuth bands on the
+// copy stream (band k = rows [k*rows, (k+1)*rows) of each image), and
+// chunkEv[k] marks band k of both images resident, so complex matching of the
+// points whose windows lie in bands <= k overlaps the copies of later bands.
+// Device-resident images are used in place.  rows[i] = 0 for a device image.
+struct Bands {
+    int nb = 1;
+    int rows[2] = {0, 0};
+};
+static int upload_banded(sb_context* c, const sb_image* im[2], const void* dptr[2], Bands* b)
+{
+    size_t hostBytes = 0;
+    for (int i = 0; i < 2; ++i) {
+        const size_t elem = im[i]->sampleType == SB_CFLOAT32 ? 8 : 4;
+        if (!im[i]->onDevice) hostBytes += (size_t)im[i]->nr * (size_t)im[i]->na * elem;
+    }
+    // about 8 MB per band and image, at most SB_MAX_BANDS bands
+    size_t nb = hostBytes / ((size_t)16 << 20);
+    b->nb = nb < 1 ? 1 : (nb > (size_t)SB_MAX_BANDS ? SB_MAX_BANDS : (int)nb);
+    cudaError_t e;
+    // the copy stream must not overtake work still reading these buffers
+    cudaEventRecord(c->chunkEv[0], c->stream);
+    cudaStreamWaitEvent(c->copyStream, c->chunkEv[0], 0);
+    char* dst[2] = {nullptr, nullptr};
+    for (int i = 0; i < 2; ++i) {
+        if (im[i]->onDevice) {
+            dptr[i] = im[i]->data;
+            b->rows[i] = 0;
+            continue;
+        }
+        const size_t elem = im[i]->sampleType == SB_CFLOAT32 ? 8 : 4;
+        const size_t bytes = (size_t)im[i]->nr * (size_t)im[i]->na * elem;
+        dst[i] = (char*)sb_ctx_buf(c, i == 0 ? "img1" : "img2", bytes, &e);
+        if (!dst[i]) return sb_ctx_cuda(c, e, "cudaMalloc(image)");
+        dptr[i] = dst[i];
+        b->rows[i] = (im[i]->na + b->nb - 1) / b->nb;
+    }
+    for (int k = 0; k < b->nb; ++k) {
+        for (int i = 0; i < 2; ++i) {
+            if (!dst[i]) continue;
+            const size_t elem = im[i]->sampleType == SB_CFLOAT32 ? 8 : 4;
+            const size_t rowBytes = (size_t)im[i]->nr * elem;
+            const int r0 = k * b->rows[i];
+            const int r1 = (k + 1) * b->rows[i] < im[i]->na ? (k + 1) * b->rows[i] : im[i]->na;
+            if (r1 <= r0) continue;
+            e = cudaMemcpyAsync(dst[i] + (size_t)r0 * rowBytes, (const char*)im[i]->data + (size_t)r0 * rowBytes,
+                                (size_t)(r1 - r0) * rowBytes, cudaMemcpyHostToDevice, c->copyStream);
+            if (e != cudaSuccess) return sb_ctx_cuda(c, e, "cudaMemcpyAsync(image band)");
+        }
+        cudaEventRecord(c->chunkEv[k], c->copyStream);
+    }
+    return SB_OK;
+}
+
 static int check_image(sb_context* c, const sb_image* im)
 {
     if (!im || !im->data || im->nr <= 0 || im->na <= 0) return sb_ctx_fail(c, SB_ERR_ARG, "invalid image");
@@ -459,11 +522,6 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
     const bool devPlan = p->polyShift != 0;
     std::vector<PointPlan> plan;
     std::vector<int> clist;
-    if (!devPlan) plan_strack(p, img1->nr, img1->na, img2->nr, img2->na, plan, clist);
-
-    const void *d1, *d2;
-    if ((rc = sb_image_to_device(c, img1, "img1", &d1)) != SB_OK) return rc;
-    if ((rc = sb_image_to_device(c, img2, "img2", &d2)) != SB_OK) return rc;
     cudaError_t e;
     PointPlan* dplan = (PointPlan*)sb_ctx_buf(c, "plan", sizeof(PointPlan) * n, &e);
     PointRec* drec = (PointRec*)sb_ctx_buf(c, "rec", sizeof(PointRec) * n, &e);
@@ -476,8 +534,20 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
     float* dC = (float*)sb_ctx_buf(c, "corr", sizeof(float) * n, &e);
     float* dZ = (float*)sb_ctx_buf(c, "azd", sizeof(float) * n, &e);
     uint8_t* dT = (uint8_t*)sb_ctx_buf(c, "type", n, &e);
-    if (!dplan || !drec || !dlist || !dfit || !dcount || !dstats || !dR || !dA || !dC || !dZ || !dT)
+    int* dlist2 = (int*)sb_ctx_buf(c, "listBands", sizeof(int) * (n + 1), &e);
+    int* dband = (int*)sb_ctx_buf(c, "bandOf", sizeof(int) * (n + 1), &e);
+    int* dbandCnt = (int*)sb_ctx_buf(c, "bandCount", sizeof(int) * 2 * SB_MAX_BANDS, &e);
+    if (!dplan || !drec || !dlist || !dfit || !dcount || !dstats || !dR || !dA || !dC || !dZ || !dT || !dlist2 ||
+        !dband || !dbandCnt)
         return sb_ctx_fail(c, SB_ERR_NOMEM, "device allocation failed");
+    // images: banded upload on the copy stream, overlapping the planning and
+    // the complex matching of earlier bands
+    const sb_image* ims[2] = {img1, img2};
+    const void* dimg[2] = {nullptr, nullptr};
+    Bands bands;
+    if ((rc = upload_banded(c, ims, dimg, &bands)) != SB_OK) return rc;
+    const void *d1 = dimg[0], *d2 = dimg[1];
+    if (!devPlan) plan_strack(p, img1->nr, img1->na, img2->nr, img2->na, plan, clist);
     int nC = 0;
     if (devPlan) {
         PlanArgs pa;
@@ -563,11 +633,41 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
             return sb_ctx_fail(c, SB_ERR_NOMEM, "table allocation failed");
         int bpsm = cmplx_blocks_per_sm(W);
         if (bpsm <= 0) return sb_ctx_fail(c, SB_ERR_CUDA, "complex kernel cannot be resident (W=%d)", W);
-        int nCta = c->numSM * bpsm;
-        if (nCta > a.nList) nCta = a.nList;
+        // per-band sub-lists (one band: the list as planned)
+        std::vector<int> bandOff(bands.nb + 1, 0);
+        bandOff[1] = nC;
+        if (bands.nb > 1) {
+            int hc[SB_MAX_BANDS];
+            CK(cudaMemsetAsync(dbandCnt, 0, sizeof(int) * SB_MAX_BANDS, c->stream), "memset");
+            CK(launch_band_count(dplan, dlist, nC, W, bands.rows[0], bands.rows[1], bands.nb, dband, dbandCnt,
+                                 c->stream),
+               "band_count");
+            c->launches++;
+            CK(cudaMemcpyAsync(hc, dbandCnt, sizeof(int) * bands.nb, cudaMemcpyDeviceToHost, c->stream), "count");
+            CK(cudaStreamSynchronize(c->stream), "sync");
+            for (int k = 0; k < bands.nb; ++k) bandOff[k + 1] = bandOff[k] + hc[k];
+            CK(cudaMemcpyAsync(dbandCnt + SB_MAX_BANDS, bandOff.data(), sizeof(int) * bands.nb,
+                               cudaMemcpyHostToDevice, c->stream),
+               "offsets");
+            CK(launch_band_scatter(dlist, dband, nC, bands.nb, dbandCnt + SB_MAX_BANDS, dlist2, c->stream),
+               "band_scatter");
+            c->launches++;
+            a.list = dlist2;
+        }
+        const int nBand = bands.nb > 1 ? bands.nb : 1;
         cudaEventRecord(c->sev[0], c->stream);
-        CK(launch_strack_cmplx(W, a, nCta, c->stream), "strack_cmplx");
-        c->launches++;
+        for (int k = 0; k < nBand; ++k) {
+            const int cnt = bandOff[k + 1] - bandOff[k];
+            if (cnt == 0) continue;
+            CK(cudaStreamWaitEvent(c->stream, c->chunkEv[k], 0), "wait band");
+            CmplxArgs ak = a;
+            ak.list = a.list + bandOff[k];
+            ak.fit = dfit + bandOff[k];
+            ak.nList = cnt;
+            const int nCta = c->numSM * bpsm < cnt ? c->numSM * bpsm : cnt;
+            CK(launch_strack_cmplx(W, ak, nCta, c->stream), "strack_cmplx");
+            c->launches++;
+        }
         cudaEventRecord(c->sev[1], c->stream);
         FitArgs f = make_fit_args(p, dfit, a.nList, 0, drec);
         CK(launch_strack_fit(f, c->stream), "strack_fit");
@@ -575,6 +675,8 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
         cudaEventRecord(c->sev[2], c->stream);
         c->stage[5] = (float)a.nList;
     }
+    // every band resident before the amplitude tries
+    CK(cudaStreamWaitEvent(c->stream, c->chunkEv[bands.nb - 1], 0), "wait bands");
     WalkParams w;
     w.wR = p->wR; w.wA = p->wA; w.wRa = p->wRa; w.wAa = p->wAa;
     w.noComplex = p->noComplex;

@@ -13,6 +13,8 @@ struct DevBuf {
     size_t bytes = 0;
 };
 
+constexpr int SB_MAX_BANDS = 16;  // equals sbk::SB_BANDS_MAX
+
 struct sb_context {
     int device = 0;
     int numSM = 0;
@@ -22,6 +24,8 @@ struct sb_context {
     float timing[4] = {0, 0, 0, 0};
     float stage[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     cudaEvent_t sev[16] = {};  // per-stage event pairs
+    cudaStream_t copyStream = nullptr;  // host -> device image bands
+    cudaEvent_t chunkEv[SB_MAX_BANDS] = {};  // band k of both images is resident
     int nsev = 0;
     int64_t launches = 0;
     std::string err;

@@ -165,6 +165,72 @@ cudaError_t launch_plan_poly(const PlanArgs& a, PointPlan* plan, int* clist, int
     return cudaGetLastError();
 }
 
+// Band of a complex-list point: the last image band (rows[i] rows each) its
+// two W x W windows reach; rows[i] = 0 for an image already on the device.
+__device__ __forceinline__ int point_band(const PointPlan& pl, int W, int rows1, int rows2, int nb)
+{
+    int b = 0;
+    if (rows1 > 0) b = max(b, (pl.a1 + W - 1) / rows1);
+    if (rows2 > 0) b = max(b, (pl.a2 + W - 1) / rows2);
+    return min(max(b, 0), nb - 1);
+}
+
+// Per-band point counts (block histogram, one global add per band and block).
+__global__ void band_count_kernel(const PointPlan* plan, const int* list, int n, int W, int rows1, int rows2, int nb,
+                                  int* bandOf, int* counts)
+{
+    __shared__ int h[SB_BANDS_MAX];
+    if (threadIdx.x < SB_BANDS_MAX) h[threadIdx.x] = 0;
+    __syncthreads();
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int b = point_band(plan[list[i]], W, rows1, rows2, nb);
+        bandOf[i] = b;
+        atomicAdd(&h[b], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < nb && h[threadIdx.x] > 0) atomicAdd(&counts[threadIdx.x], h[threadIdx.x]);
+}
+
+// Scatter of the list into band order; cursor[b] starts at band b's offset.
+// Positions within a band follow no particular order (every point is
+// matched independently of its list position).
+__global__ void band_scatter_kernel(const int* list, const int* bandOf, int n, int nb, int* cursor, int* out)
+{
+    __shared__ int h[SB_BANDS_MAX], base[SB_BANDS_MAX];
+    for (int t0 = blockIdx.x * blockDim.x; t0 < n; t0 += gridDim.x * blockDim.x) {
+        if (threadIdx.x < SB_BANDS_MAX) h[threadIdx.x] = 0;
+        __syncthreads();
+        const int i = t0 + threadIdx.x;
+        int b = -1, r = 0;
+        if (i < n) {
+            b = bandOf[i];
+            r = atomicAdd(&h[b], 1);
+        }
+        __syncthreads();
+        if (threadIdx.x < nb) base[threadIdx.x] = h[threadIdx.x] > 0 ? atomicAdd(&cursor[threadIdx.x], h[threadIdx.x]) : 0;
+        __syncthreads();
+        if (b >= 0) out[base[b] + r] = list[i];
+        __syncthreads();
+    }
+}
+
+cudaError_t launch_band_count(const PointPlan* plan, const int* list, int n, int W, int rows1, int rows2, int nb,
+                              int* bandOf, int* counts, cudaStream_t st)
+{
+    if (nb < 1 || nb > SB_BANDS_MAX) return cudaErrorInvalidValue;
+    const int g = min((n + 255) / 256, 1184);
+    band_count_kernel<<<g, 256, 0, st>>>(plan, list, n, W, rows1, rows2, nb, bandOf, counts);
+    return cudaGetLastError();
+}
+cudaError_t launch_band_scatter(const int* list, const int* bandOf, int n, int nb, int* cursor, int* out,
+                                cudaStream_t st)
+{
+    if (nb < 1 || nb > SB_BANDS_MAX) return cudaErrorInvalidValue;
+    const int g = min((n + 255) / 256, 1184);
+    band_scatter_kernel<<<g, 256, 0, st>>>(list, bandOf, n, nb, cursor, out);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_rec_init(PointRec* rec, int n, cudaStream_t st)
 {
     rec_init_kernel<<<(n + 255) / 256, 256, 0, st>>>(rec, n);
