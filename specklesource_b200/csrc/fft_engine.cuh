@@ -18,8 +18,9 @@
 // Register DFTs of composite size R are built at compile time by splitting off
 // the smallest prime factor; prime factors use the direct sum.  Twiddles come
 // from a table W_TN^e = exp(-2 pi i e/TN), e < TN, read with compile-time
-// indices (uniform across the warp, so broadcast); factors of +-1, +-i are
-// applied without a multiply.
+// indices (uniform across the warp, so broadcast) for the inter-step twiddles,
+// while the twiddles inside the register DFTs are compile-time constants;
+// factors of +-1, +-i are applied without a multiply.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -44,6 +45,54 @@ constexpr int smallest_factor(int n)
     return n;
 }
 
+// ---------------------------------------------------------------- compile-time twiddles
+// cos and sin of 2 pi e / n for integers, evaluated by the compiler: octant
+// reduction with exact integer arithmetic, then the Taylor series of sin and
+// cos on [0, pi/4] in double (14 terms: truncation below 1e-20), rounded once
+// to float where used.  Compile-time twiddles become immediate operands.
+struct CxPair {
+    double c, s;
+};
+constexpr double kQuarterPi = 0.78539816339744830961566084581987572;
+__host__ __device__ constexpr double cx_sin(double x)
+{
+    double term = x, sum = x;
+    for (int k = 1; k < 14; ++k) {
+        term *= -x * x / ((2.0 * k) * (2.0 * k + 1.0));
+        sum += term;
+    }
+    return sum;
+}
+__host__ __device__ constexpr double cx_cos(double x)
+{
+    double term = 1.0, sum = 1.0;
+    for (int k = 1; k < 14; ++k) {
+        term *= -x * x / ((2.0 * k - 1.0) * (2.0 * k));
+        sum += term;
+    }
+    return sum;
+}
+__host__ __device__ constexpr CxPair cx_cossin(int e, int n)  // (cos, sin)(2 pi e / n)
+{
+    const long long r = ((e % n) + n) % n;
+    const long long m = 8 * r;                  // theta / (pi/4) = m / n
+    const int oct = (int)(m / n);
+    const long long fnum = m - (long long)oct * n;  // phi = (pi/4) fnum / n
+    const double phi = kQuarterPi * (double)fnum / (double)n;
+    const double psi = kQuarterPi * (double)(n - fnum) / (double)n;  // pi/4 - phi
+    const double Sp = cx_sin(phi), Cp = cx_cos(phi), Sq = cx_sin(psi), Cq = cx_cos(psi);
+    switch (oct) {
+    case 0: return {Cp, Sp};
+    case 1: return {Sq, Cq};
+    case 2: return {-Sp, Cp};
+    case 3: return {-Cq, Sq};
+    case 4: return {-Cp, -Sp};
+    case 5: return {-Sq, -Cq};
+    case 6: return {Sp, -Cp};
+    default: return {Cq, -Sq};
+    }
+}
+
 // v * W_TN^{E} for the direction DIR (W = exp(DIR * 2 pi i / TN)); E reduced mod TN.
 template <int E, int TN, int DIR>
 __device__ __forceinline__ float2 twmul(float2 v, const float2* __restrict__ tw)
@@ -59,9 +108,10 @@ __device__ __forceinline__ float2 twmul(float2 v, const float2* __restrict__ tw)
     } else if constexpr (4 * e == 3 * TN) {
         return DIR > 0 ? make_float2(v.y, -v.x) : make_float2(-v.y, v.x);
     } else {
-        float2 w = tw[e];  // table holds the forward (DIR=-1) twiddle
-        if (DIR > 0) w.y = -w.y;
-        return cmul(v, w);
+        constexpr CxPair w = cx_cossin(e, TN);
+        constexpr float wr = (float)w.c;
+        constexpr float wi = (float)(DIR > 0 ? w.s : -w.s);
+        return cmul(v, make_float2(wr, wi));
     }
 }
 

@@ -29,7 +29,7 @@ struct CmplxSmem {
                                     sizeof(float) * (NFAST * NFAST) + sizeof(double) * (NT / 32) * 8 + 64;
 };
 
-// |c| of the 2W x 2W surface at unshifted index (cy, cx).  The parity plane
+// |c|^2 of the 2W x 2W surface at unshifted index (cy, cx).  The parity plane
 // (e1, e2) = (cy & 1, cx & 1) is a W x W float array at float offset poff(q),
 // q = 2 e1 + e2, from the start of shared memory (buffers X | Y | Z of 2W(W+1)
 // floats each): (0,0) X[0, W^2), (0,1) X[W^2, 2W^2), (1,0) the last W^2 floats
@@ -74,33 +74,76 @@ __device__ __forceinline__ float2 load_sample_t(const void* __restrict__ img, in
 
 // Final store of a pair of column passes of the padded inverse, parities
 // (0, E2) and (1, E2) (line l < W: e1 = 0, else e1 = 1, column l mod W):
-// |c| goes to the parity plane and the thread's running findCPeak maximum is
-// updated.  The maximum is the am_key of |c| and its position in findCPeak's
-// scan order (cpeak_rank).  The rank is folded from compile-time parts: the
-// output row is m1 = k1 + N1 k2, so cy = 2 m1 + e1 lies in the upper half
-// (cy >= W) exactly when k2 >= N2 / 2.
+// |c|^2 goes to the parity plane and the thread's running maximum of it is
+// kept.  (|c| = sqrtf(|c|^2) is taken where a value is used; the argmax over
+// |c| with findCPeak's tie order is recovered exactly afterwards, see
+// cpeak_from_planes.)  fmaxf ignores NaN, so NaN never wins.
 template <int W, int N1, int N2, int E2>
-struct MagArgmax {
+struct MagMax {
     float* plane0;  // parity (0, E2)
     float* plane1;  // parity (1, E2)
-    unsigned long long& best;
+    float& pmax;
     __device__ __forceinline__ void operator()(int l, int k1, int k2, float2 z) const
     {
-        static_assert(N2 % 2 == 0, "the half test needs an even N2");
         const int e1 = l >= W;
         const int col = l - (e1 ? W : 0);
-        const float v = sqrtf(z.x * z.x + z.y * z.y);
-        (e1 ? plane1 : plane0)[(k1 + N1 * k2) * W + col] = v;
-        const int cx = 2 * col + E2;
-        const bool xi = cx < W;  // fftshifted x >= W
-        const int j = xi ? cx : cx - W;
-        const bool yi = k2 < N2 / 2;  // fftshifted y >= W
-        const int i = 2 * k1 + e1 + 2 * N1 * k2 - (yi ? 0 : W);
-        const int q = (!yi && !xi) ? 0 : ((yi && xi) ? 1 : (yi ? 2 : 3));
-        const unsigned long long key = am_key(v, (unsigned)((i * W + j) * 4 + q));
-        best = key > best ? key : best;
+        const float p = z.x * z.x + z.y * z.y;
+        (e1 ? plane1 : plane0)[(k1 + N1 * k2) * W + col] = p;
+        pmax = fmaxf(pmax, p);
     }
 };
+
+// findCPeak (speckleTrack.c:744-805) over the four |c|^2 planes, given the
+// block maximum pmax of |c|^2: the peak is the largest |c| = sqrtf(|c|^2)
+// (> 0), ties to the first position in findCPeak's scan order (cpeak_rank).
+// sqrtf is correctly rounded and monotone, so every position whose sqrtf
+// equals sqrtf(pmax) has |c|^2 within a relative 2^-20 of pmax: only those
+// are ranked.  Returns the fftshifted (iMax, jMax), or (0, 0) when nothing is
+// above 0.  iscr: NT/32 words.
+template <int W, int NT>
+__device__ __forceinline__ void cpeak_from_planes(const float* smf, float pmax, unsigned* iscr, int& iMax, int& jMax)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    unsigned u = __reduce_max_sync(0xffffffffu, __float_as_uint(pmax));  // |c|^2 >= 0: bits order as values
+    if (lane == 0) iscr[warp] = u;
+    __syncthreads();
+    u = iscr[0];
+#pragma unroll
+    for (int w = 1; w < NT / 32; ++w) u = max(u, iscr[w]);
+    __syncthreads();
+    const float pm = __uint_as_float(u);
+    iMax = 0;
+    jMax = 0;
+    if (!(pm > 0.f)) return;  // uniform
+    const float sm = sqrtf(pm);
+    const float lo = pm * (1.0f - 1.0f / 1048576.0f);
+    unsigned best = 0xffffffffu;
+    constexpr int Q4 = W * W / 4;  // float4 per plane
+    for (int e = tid; e < 4 * Q4; e += NT) {
+        const int q = e / Q4, i4 = e - q * Q4;
+        const float4 v = reinterpret_cast<const float4*>(smf + poff<W>(q))[i4];
+        const float vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            if (vv[c] >= lo && sqrtf(vv[c]) == sm) {
+                const int idx = 4 * i4 + c;
+                const int cy = 2 * (idx / W) + (q >> 1), cx = 2 * (idx % W) + (q & 1);
+                const int y = cy < W ? cy + W : cy - W, x = cx < W ? cx + W : cx - W;
+                best = min(best, (unsigned)cpeak_rank(y, x, W));
+            }
+        }
+    }
+    best = __reduce_min_sync(0xffffffffu, best);
+    if (lane == 0) iscr[warp] = best;
+    __syncthreads();
+    best = iscr[0];
+#pragma unroll
+    for (int w = 1; w < NT / 32; ++w) best = min(best, iscr[w]);
+    __syncthreads();
+    const int q = best & 3, ij = best >> 2;
+    iMax = ij / W + ((q == 1 || q == 2) ? W : 0);
+    jMax = ij % W + ((q == 1 || q == 3) ? W : 0);
+}
 
 template <int W, int NT, bool F32>
 __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(CmplxArgs a)
@@ -254,26 +297,20 @@ __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(Cmp
         // (1,0) in place; R1 (Z) -> (0,1) into D and (1,1) in place.  Each ends
         // in |c| and the running argmax; the buffers are placed so that no pass
         // overwrites an input still needed or a finished plane.
-        unsigned long long best = 0ull;
+        float pmax = 0.f;
         {
             auto mulTau = [tau](int, int k) { return tau[k]; };
             auto colY = [Y](int l, int k) { return Y[k * RS + l]; };
             sbfft::fft_lines_dual<N1, N2, 1, W, NT, 1, RS, IMG, false>(
-                X, colY, mulTau, MagArgmax<W, N1, N2, 0>{smf + poff<W>(0), smf + poff<W>(2), best}, twW);
+                X, colY, mulTau, MagMax<W, N1, N2, 0>{smf + poff<W>(0), smf + poff<W>(2), pmax}, twW);
             float2* D = X + (W * W) / 2;  // spans the end of X and the start of Y
             auto colZ = [Z](int l, int k) { return Z[k * RS + l]; };
             sbfft::fft_lines_dual<N1, N2, 1, W, NT, 1, RS, 2 * IMG - (W * W) / 2, false>(
-                D, colZ, mulTau, MagArgmax<W, N1, N2, 1>{smf + poff<W>(1), smf + poff<W>(3), best}, twW);
+                D, colZ, mulTau, MagMax<W, N1, N2, 1>{smf + poff<W>(1), smf + poff<W>(3), pmax}, twW);
         }
         // ---------------------------------------------------- findCPeak
-        best = block_max_u64(best, reinterpret_cast<unsigned long long*>(red));
-        int iMax = 0, jMax = 0;
-        if ((best >> 32) != 0ull) {
-            const unsigned rank = 0xffffffffu - (unsigned)(best & 0xffffffffull);
-            const int q = rank & 3, ij = rank >> 2;
-            iMax = ij / W + ((q == 1 || q == 2) ? W : 0);
-            jMax = ij % W + ((q == 1 || q == 3) ? W : 0);
-        }
+        int iMax, jMax;
+        cpeak_from_planes<W, NT>(smf, pmax, reinterpret_cast<unsigned*>(red), iMax, jMax);
         double cMax;
         const bool rejected = (iMax < (NFAST / 2) || iMax > (W2 - NFAST / 2) || jMax < (NFAST / 2) ||
                                jMax > (W2 - NFAST / 2));
@@ -286,7 +323,7 @@ __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(Cmp
             // ------------------------------------------------ overSampleC on the 8x8 block
             if (tid < NFAST * NFAST) {
                 const int t1 = tid / NFAST, t2 = tid % NFAST;
-                blk[tid] = fmap<W>(smf, iMax - NFAST / 2 + t1, jMax - NFAST / 2 + t2);
+                blk[tid] = sqrtf(fmap<W>(smf, iMax - NFAST / 2 + t1, jMax - NFAST / 2 + t2));
             }
             __syncthreads();
             const ArgMax ob = oversample_peak_real<NT>(blk, osD, Yb, T, reinterpret_cast<unsigned long long*>(red));
@@ -304,9 +341,9 @@ __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(Cmp
                 const int f = tid / NGAUSS, k = tid % NGAUSS;
                 FitJob* fj = &a.fit[it];
                 if (f == 0) {
-                    fj->samp[0][k] = fmap<W>(smf, iM, jM - NGAUSS / 2 + k);
+                    fj->samp[0][k] = sqrtf(fmap<W>(smf, iM, jM - NGAUSS / 2 + k));
                 } else {
-                    fj->samp[1][k] = fmap<W>(smf, iM - NGAUSS / 2 + k, jM);
+                    fj->samp[1][k] = sqrtf(fmap<W>(smf, iM - NGAUSS / 2 + k, jM));
                 }
                 if (k == 0) fj->x0[f] = (f == 0 ? jM : iM) - NGAUSS / 2;
             }
