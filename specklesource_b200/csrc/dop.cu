@@ -11,7 +11,7 @@ namespace sbk {
 __global__ void __launch_bounds__(256) dop_kernel(const float2* p1, const float2* p2, int nAz, int nRg, int wA,
                                                   int* out)
 {
-    __shared__ double red[(256 / 32) * 8];
+    __shared__ double red[(256 / 32 + 1) * 8];
     const size_t n = (size_t)nAz * nRg;
     const float2* a = p1 + (size_t)blockIdx.x * n;
     const float2* b = p2 + (size_t)blockIdx.x * n;

@@ -29,7 +29,7 @@ struct NoallocCfg {
                                     ? sbfft::StagedTile<N>::elems
                                     : sbfft::StagedTile<WS>::elems;
     static constexpr size_t smem = sizeof(float2) * (TILE + WS + N + WS + OSW * NFAST + NFAST * OSW) +
-                                   sizeof(float) * NFAST * NFAST + sizeof(double) * (NT / 32) * 8 +
+                                   sizeof(float) * NFAST * NFAST + sizeof(double) * (NT / 32 + 1) * 8 +
                                    sizeof(int) * (3 * (NT / 32) + 8) + 64;
     // F1, F2, work (WS^2 each), z (N^2), mag (N^2 floats)
     static constexpr size_t perCta = (size_t)3 * WS * WS + (size_t)N * N + (size_t)N * N / 2;
@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(NoallocCfg<WS>::NT) amp_noalloc_kernel(Noalloc
     float2* T = osA + OSW * NFAST;
     float* blk = reinterpret_cast<float*>(T + NFAST * OSW);
     double* red = reinterpret_cast<double*>(blk + NFAST * NFAST);
-    int* isc = reinterpret_cast<int*>(red + (NT / 32) * 8);
+    int* isc = reinterpret_cast<int*>(red + (NT / 32 + 1) * 8);
     const int tid = threadIdx.x;
 
     // constant tables (forward twiddles, parity twiddles, oversampling matrix)

@@ -30,7 +30,7 @@ struct AmpCfg {
                                     ? sbfft::StagedTile<N>::elems
                                     : sbfft::StagedTile<WS>::elems;
     static constexpr size_t smem = sizeof(float2) * (TILE + WS + N + WS + OSW * NFAST + NFAST * OSW) +
-                                   sizeof(float) * NFAST * NFAST + sizeof(double) * (NT / 32) * 8 +
+                                   sizeof(float) * NFAST * NFAST + sizeof(double) * (NT / 32 + 1) * 8 +
                                    sizeof(int) * (3 * (NT / 32) + 8) + 64;
     // workspace: F1, F2, work (Ws^2 each), z (N^2), mag (N^2 floats)
     static constexpr size_t scratch = (size_t)3 * WS * WS + (size_t)N * N + (size_t)N * N / 2;
@@ -50,7 +50,7 @@ __global__ void __launch_bounds__(AmpCfg<WS>::NT) strack_amp_kernel(AmpArgs a)
     float2* T = osA + OSW * NFAST;
     float* blk = reinterpret_cast<float*>(T + NFAST * OSW);
     double* red = reinterpret_cast<double*>(blk + NFAST * NFAST);
-    int* isc = reinterpret_cast<int*>(red + (NT / 32) * 8);
+    int* isc = reinterpret_cast<int*>(red + (NT / 32 + 1) * 8);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
     for (int e = tid; e < WS; e += NT) {

@@ -26,7 +26,7 @@ struct CmplxSmem {
     static constexpr int IMG = W * RS;  // float2 per buffer; three buffers X, Y, Z
     static constexpr int OSD = OSW * NFAST / 2 + 16;  // float2 of the real oversampling table
     static constexpr size_t bytes = sizeof(float2) * (3 * IMG + 2 * W + OSD + NFAST * NFAST + NFAST * OSW) +
-                                    sizeof(float) * (NFAST * NFAST) + sizeof(double) * (NT / 32) * 8 + 64;
+                                    sizeof(float) * (NFAST * NFAST) + sizeof(double) * (NT / 32 + 1) * 8 + 64;
 };
 
 // |c|^2 of the 2W x 2W surface at unshifted index (cy, cx).  The parity plane

@@ -21,10 +21,14 @@ __device__ __forceinline__ double warp_allsum(double v)
 }
 
 // Sum K doubles over the block; every thread gets the totals.
-// red: shared scratch of (NT/32)*K doubles.
+// red: shared scratch of (NT/32 + 1)*K doubles.  Warp sums by shuffles, the
+// cross-warp sum by warp 0 alone (the totals get their own slots, so the
+// scratch may be reused by the next call without a third barrier).
 template <int K, int NT>
 __device__ __forceinline__ void block_allsum(double (&v)[K], double* red)
 {
+    constexpr int NW = NT / 32;
+    static_assert(NW >= 1 && NW <= 32, "one to 32 warps");
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int k = 0; k < K; ++k) v[k] = warp_allsum(v[k]);
@@ -33,14 +37,25 @@ __device__ __forceinline__ void block_allsum(double (&v)[K], double* red)
         for (int k = 0; k < K; ++k) red[warp * K + k] = v[k];
     }
     __syncthreads();
+    if (warp == 0) {
+        double t[K];
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-        double s = 0.0;
+        for (int k = 0; k < K; ++k) t[k] = lane < NW ? red[lane * K + k] : 0.0;
 #pragma unroll
-        for (int w = 0; w < NT / 32; ++w) s += red[w * K + k];
-        v[k] = s;
+        for (int o = 16; o > 0; o >>= 1) {
+            if (o < NW) {
+#pragma unroll
+                for (int k = 0; k < K; ++k) t[k] += __shfl_xor_sync(0xffffffffu, t[k], o);
+            }
+        }
+        if (lane == 0) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) red[NW * K + k] = t[k];
+        }
     }
     __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = red[NW * K + k];
 }
 
 // (value, rank) maximum: larger value wins, equal values -> smaller rank.

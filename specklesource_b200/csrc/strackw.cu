@@ -114,7 +114,7 @@ struct SwCfg {
                                     ? sbfft::StagedTile<N>::elems
                                     : sbfft::StagedTile<W>::elems;
     static constexpr size_t smem = sizeof(float2) * (TILE + W + N + W) + sizeof(double) * (W_OSW * W_N1) +
-                                   sizeof(double) * (W_N1 * W_N1 + W_N1 * W_OSW) + sizeof(double) * (NT / 32) * 8 +
+                                   sizeof(double) * (W_N1 * W_N1 + W_N1 * W_OSW) + sizeof(double) * (NT / 32 + 1) * 8 +
                                    sizeof(int) * (3 * (NT / 32) + 8) + 64;
     static_assert((NT / 32) * 2 * N <= W * W, "per-warp prefix slices must fit in `work`");
     // workspace (float2 units): F1, F2, work (W^2 each), I1, I2 (N^2 floats
@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(SwCfg<W>::NT) strackw_kernel(SwArgs a)
     double* X = Bm + W_OSW * W_N1;                          // 21 x 21 block
     double* T = X + W_N1 * W_N1;                            // 21 x 64
     double* red = T + W_N1 * W_OSW;
-    int* isc = reinterpret_cast<int*>(red + (NT / 32) * 8);
+    int* isc = reinterpret_cast<int*>(red + (NT / 32 + 1) * 8);
     const int tid = threadIdx.x;
 
     for (int e = tid; e < W; e += NT) {
