@@ -24,6 +24,7 @@
 #include "capi_internal.h"
 #include "strack_device.cuh"
 #include "strack_finalize.h"
+#include "partition.h"
 #include "strack_fit.h"
 #include "strack_kernels.h"
 
@@ -527,7 +528,6 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
     PointRec* drec = (PointRec*)sb_ctx_buf(c, "rec", sizeof(PointRec) * n, &e);
     int* dlist = (int*)sb_ctx_buf(c, "list", sizeof(int) * (n + 1), &e);
     FitJob* dfit = (FitJob*)sb_ctx_buf(c, "fit", sizeof(FitJob) * (n + 1), &e);
-    int* dcount = (int*)sb_ctx_buf(c, "count", sizeof(int) * 4, &e);
     unsigned long long* dstats = (unsigned long long*)sb_ctx_buf(c, "stats", sizeof(unsigned long long) * 8, &e);
     float* dR = (float*)sb_ctx_buf(c, "offR", sizeof(float) * n, &e);
     float* dA = (float*)sb_ctx_buf(c, "offA", sizeof(float) * n, &e);
@@ -535,10 +535,10 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
     float* dZ = (float*)sb_ctx_buf(c, "azd", sizeof(float) * n, &e);
     uint8_t* dT = (uint8_t*)sb_ctx_buf(c, "type", n, &e);
     int* dlist2 = (int*)sb_ctx_buf(c, "listBands", sizeof(int) * (n + 1), &e);
-    int* dband = (int*)sb_ctx_buf(c, "bandOf", sizeof(int) * (n + 1), &e);
-    int* dbandCnt = (int*)sb_ctx_buf(c, "bandCount", sizeof(int) * 2 * SB_MAX_BANDS, &e);
-    if (!dplan || !drec || !dlist || !dfit || !dcount || !dstats || !dR || !dA || !dC || !dZ || !dT || !dlist2 ||
-        !dband || !dbandCnt)
+    int* dkey = (int*)sb_ctx_buf(c, "listKey", sizeof(int) * (n + 1), &e);
+    int* dpart = (int*)sb_ctx_buf(c, "partScratch", sizeof(int) * partition_scratch_ints(n, PART_KMAX), &e);
+    if (!dplan || !drec || !dlist || !dfit || !dstats || !dR || !dA || !dC || !dZ || !dT || !dlist2 ||
+        !dkey || !dpart)
         return sb_ctx_fail(c, SB_ERR_NOMEM, "device allocation failed");
     // images: banded upload on the copy stream, overlapping the planning and
     // the complex matching of earlier bands
@@ -571,10 +571,12 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
             pa.mR0 = p->mask->r0; pa.mA0 = p->mask->a0; pa.mNr = p->mask->nr; pa.mNa = p->mask->na;
             pa.mNrl = p->mask->nrl; pa.mNal = p->mask->nal;
         }
-        CK(cudaMemsetAsync(dcount, 0, sizeof(int), c->stream), "memset");
-        CK(launch_plan_poly(pa, dplan, dlist, dcount, c->stream), "plan_poly");
-        c->launches++;
-        CK(cudaMemcpyAsync(&nC, dcount, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "count");
+        CK(launch_plan_poly(pa, dplan, dkey, c->stream), "plan_poly");
+        CK(launch_partition(dkey, nullptr, n, 1, dlist, dpart, c->stream), "partition");
+        c->launches += 4;
+        CK(cudaMemcpyAsync(&nC, dpart + partition_keyoff_at(n, 1) + 1, sizeof(int), cudaMemcpyDeviceToHost,
+                           c->stream),
+           "count");
         CK(cudaStreamSynchronize(c->stream), "sync");
     } else {
         CK(cudaMemcpyAsync(dplan, plan.data(), sizeof(PointPlan) * n, cudaMemcpyHostToDevice, c->stream), "plan");
@@ -637,21 +639,14 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
         std::vector<int> bandOff(bands.nb + 1, 0);
         bandOff[1] = nC;
         if (bands.nb > 1) {
-            int hc[SB_MAX_BANDS];
-            CK(cudaMemsetAsync(dbandCnt, 0, sizeof(int) * SB_MAX_BANDS, c->stream), "memset");
-            CK(launch_band_count(dplan, dlist, nC, W, bands.rows[0], bands.rows[1], bands.nb, dband, dbandCnt,
-                                 c->stream),
-               "band_count");
-            c->launches++;
-            CK(cudaMemcpyAsync(hc, dbandCnt, sizeof(int) * bands.nb, cudaMemcpyDeviceToHost, c->stream), "count");
-            CK(cudaStreamSynchronize(c->stream), "sync");
-            for (int k = 0; k < bands.nb; ++k) bandOff[k + 1] = bandOff[k] + hc[k];
-            CK(cudaMemcpyAsync(dbandCnt + SB_MAX_BANDS, bandOff.data(), sizeof(int) * bands.nb,
-                               cudaMemcpyHostToDevice, c->stream),
+            CK(launch_band_key(dplan, dlist, nC, W, bands.rows[0], bands.rows[1], bands.nb, dkey, c->stream),
+               "band_key");
+            CK(launch_partition(dkey, dlist, nC, bands.nb, dlist2, dpart, c->stream), "partition");
+            c->launches += 4;
+            CK(cudaMemcpyAsync(bandOff.data(), dpart + partition_keyoff_at(nC, bands.nb),
+                               sizeof(int) * (bands.nb + 1), cudaMemcpyDeviceToHost, c->stream),
                "offsets");
-            CK(launch_band_scatter(dlist, dband, nC, bands.nb, dbandCnt + SB_MAX_BANDS, dlist2, c->stream),
-               "band_scatter");
-            c->launches++;
+            CK(cudaStreamSynchronize(c->stream), "sync");
             a.list = dlist2;
         }
         const int nBand = bands.nb > 1 ? bands.nb : 1;
@@ -692,11 +687,13 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
         c->stage[3] += t1;
     }
     for (int stage = 1; stage <= 2 && stage <= p->maxTries; ++stage) {
-        CK(cudaMemsetAsync(dcount, 0, sizeof(int), c->stream), "memset");
-        CK(launch_select(dplan, drec, n, w, stage, dlist, dcount, c->stream), "select");
-        c->launches++;
+        CK(launch_select(dplan, drec, n, w, stage, dkey, c->stream), "select");
+        CK(launch_partition(dkey, nullptr, n, 1, dlist, dpart, c->stream), "partition");
+        c->launches += 4;
         int cnt = 0;
-        CK(cudaMemcpyAsync(&cnt, dcount, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "count");
+        CK(cudaMemcpyAsync(&cnt, dpart + partition_keyoff_at(n, 1) + 1, sizeof(int), cudaMemcpyDeviceToHost,
+                           c->stream),
+           "count");
         CK(cudaStreamSynchronize(c->stream), "sync");
         if (cnt == 0) continue;
         const int Ws = WA * (stage == 1 ? 1 : LA);

@@ -22,17 +22,15 @@ __global__ void rec_init_kernel(PointRec* rec, int n)
     rec[p] = r;
 }
 
-// Appends to `list` the points whose next missing try is `stage`.
+// key[p] = 0 for the points whose next missing try is `stage`, else -1 (the
+// list is then built in raster order by the ordered partition).
 __global__ void select_stage_kernel(const PointPlan* plan, const PointRec* rec, int n, WalkParams w, int stage,
-                                    int* list, int* count)
+                                    int* key)
 {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
     const WalkOut o = strack_walk(plan[p], rec[p], w);
-    if (o.stage_next == stage) {
-        const int k = atomicAdd(count, 1);
-        list[k] = p;
-    }
+    key[p] = o.stage_next == stage ? 0 : -1;
 }
 
 // azShift in effect at each point = the last value set at or before it in
@@ -111,8 +109,8 @@ __global__ void finalize_kernel(const PointPlan* plan, const PointRec* rec, int 
 // independent: findImage2Pos (speckleTrack.c:810-847, the polyShift branch),
 // maskValue (:1951-1965) and boundsCheck (:1822-1828) for the three windows.
 // Products and sums are rounded separately (no fused multiply-add), as on the
-// host.  Complex candidates are appended to clist.
-__global__ void plan_poly_kernel(PlanArgs a, PointPlan* plan, int* clist, int* ccount)
+// host.  key[p] = 0 for complex candidates, else -1.
+__global__ void plan_poly_kernel(PlanArgs a, PointPlan* plan, int* key)
 {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= a.nR * a.nA) return;
@@ -155,13 +153,13 @@ __global__ void plan_poly_kernel(PlanArgs a, PointPlan* plan, int* clist, int* c
             pl.flags |= (s == 1 ? PF_SBOUND : PF_LBOUND);
     }
     plan[p] = pl;
-    if ((pl.flags & PF_CBOUND) && (pl.flags & PF_MASK) && a.noComplex == 0) clist[atomicAdd(ccount, 1)] = p;
+    key[p] = ((pl.flags & PF_CBOUND) && (pl.flags & PF_MASK) && a.noComplex == 0) ? 0 : -1;
 }
 
-cudaError_t launch_plan_poly(const PlanArgs& a, PointPlan* plan, int* clist, int* ccount, cudaStream_t st)
+cudaError_t launch_plan_poly(const PlanArgs& a, PointPlan* plan, int* key, cudaStream_t st)
 {
     const int n = a.nR * a.nA;
-    plan_poly_kernel<<<(n + 255) / 256, 256, 0, st>>>(a, plan, clist, ccount);
+    plan_poly_kernel<<<(n + 255) / 256, 256, 0, st>>>(a, plan, key);
     return cudaGetLastError();
 }
 
@@ -175,59 +173,20 @@ __device__ __forceinline__ int point_band(const PointPlan& pl, int W, int rows1,
     return min(max(b, 0), nb - 1);
 }
 
-// Per-band point counts (block histogram, one global add per band and block).
-__global__ void band_count_kernel(const PointPlan* plan, const int* list, int n, int W, int rows1, int rows2, int nb,
-                                  int* bandOf, int* counts)
+// Band key of every complex-list entry (for the ordered partition by band).
+__global__ void band_key_kernel(const PointPlan* plan, const int* list, int n, int W, int rows1, int rows2, int nb,
+                                int* bandOf)
 {
-    __shared__ int h[SB_BANDS_MAX];
-    if (threadIdx.x < SB_BANDS_MAX) h[threadIdx.x] = 0;
-    __syncthreads();
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int b = point_band(plan[list[i]], W, rows1, rows2, nb);
-        bandOf[i] = b;
-        atomicAdd(&h[b], 1);
-    }
-    __syncthreads();
-    if (threadIdx.x < nb && h[threadIdx.x] > 0) atomicAdd(&counts[threadIdx.x], h[threadIdx.x]);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) bandOf[i] = point_band(plan[list[i]], W, rows1, rows2, nb);
 }
 
-// Scatter of the list into band order; cursor[b] starts at band b's offset.
-// Positions within a band follow no particular order (every point is
-// matched independently of its list position).
-__global__ void band_scatter_kernel(const int* list, const int* bandOf, int n, int nb, int* cursor, int* out)
-{
-    __shared__ int h[SB_BANDS_MAX], base[SB_BANDS_MAX];
-    for (int t0 = blockIdx.x * blockDim.x; t0 < n; t0 += gridDim.x * blockDim.x) {
-        if (threadIdx.x < SB_BANDS_MAX) h[threadIdx.x] = 0;
-        __syncthreads();
-        const int i = t0 + threadIdx.x;
-        int b = -1, r = 0;
-        if (i < n) {
-            b = bandOf[i];
-            r = atomicAdd(&h[b], 1);
-        }
-        __syncthreads();
-        if (threadIdx.x < nb) base[threadIdx.x] = h[threadIdx.x] > 0 ? atomicAdd(&cursor[threadIdx.x], h[threadIdx.x]) : 0;
-        __syncthreads();
-        if (b >= 0) out[base[b] + r] = list[i];
-        __syncthreads();
-    }
-}
-
-cudaError_t launch_band_count(const PointPlan* plan, const int* list, int n, int W, int rows1, int rows2, int nb,
-                              int* bandOf, int* counts, cudaStream_t st)
+cudaError_t launch_band_key(const PointPlan* plan, const int* list, int n, int W, int rows1, int rows2, int nb,
+                            int* bandOf, cudaStream_t st)
 {
     if (nb < 1 || nb > SB_BANDS_MAX) return cudaErrorInvalidValue;
-    const int g = min((n + 255) / 256, 1184);
-    band_count_kernel<<<g, 256, 0, st>>>(plan, list, n, W, rows1, rows2, nb, bandOf, counts);
-    return cudaGetLastError();
-}
-cudaError_t launch_band_scatter(const int* list, const int* bandOf, int n, int nb, int* cursor, int* out,
-                                cudaStream_t st)
-{
-    if (nb < 1 || nb > SB_BANDS_MAX) return cudaErrorInvalidValue;
-    const int g = min((n + 255) / 256, 1184);
-    band_scatter_kernel<<<g, 256, 0, st>>>(list, bandOf, n, nb, cursor, out);
+    if (n == 0) return cudaSuccess;
+    band_key_kernel<<<(n + 255) / 256, 256, 0, st>>>(plan, list, n, W, rows1, rows2, nb, bandOf);
     return cudaGetLastError();
 }
 
@@ -237,9 +196,9 @@ cudaError_t launch_rec_init(PointRec* rec, int n, cudaStream_t st)
     return cudaGetLastError();
 }
 cudaError_t launch_select(const PointPlan* plan, const PointRec* rec, int n, const WalkParams& w, int stage,
-                          int* list, int* count, cudaStream_t st)
+                          int* key, cudaStream_t st)
 {
-    select_stage_kernel<<<(n + 255) / 256, 256, 0, st>>>(plan, rec, n, w, stage, list, count);
+    select_stage_kernel<<<(n + 255) / 256, 256, 0, st>>>(plan, rec, n, w, stage, key);
     return cudaGetLastError();
 }
 cudaError_t launch_az_fill(const PointRec* rec, int n, int* azEff, cudaStream_t st)
