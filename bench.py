@@ -14,6 +14,9 @@ e2e   : patches/s through the C ABI with big-endian host images in pinned
         memory; every step copies both images host->device and the five
         output grids device->host inside the timed region.
 Inputs (4.6 GB) are far larger than L2 (126 MB), so no flush is needed.
+accuracy: the last step's offsets against the FP64 oracle on a spread sample
+        of grid rows (one per host core): error percentiles in px, the
+        fraction within 0.02 px (0.01 px for complex matches), match agreement.
 Under torchrun every rank tracks its own pair (weak scaling, no collective on
 the data path); rank 0 prints the max-over-ranks time.
 """
@@ -35,6 +38,9 @@ W = 64
 GRID = dict(rStart=96, aStart=96, deltaR=24, deltaA=6, wR=W, wA=W, wRa=W, wAa=W)
 N_R = (NR - 2 * GRID["rStart"]) // GRID["deltaR"] + 1  # 993
 N_A = (NA - 2 * GRID["aStart"]) // GRID["deltaA"] + 1  # 1969
+
+
+METRIC = "patches/s at <=0.02 px err vs FP64 oracle (plain FP32); p50/p99 ms"
 
 
 def use_small_workload():
@@ -148,44 +154,101 @@ def fp32_peak_tflops(torch):
 # ---------------------------------------------------------------- CPU baseline
 
 def _cpu_worker(args):
-    band1, band2, aStart, nA = args
+    band1, band2, aStart, nA, precision = args
     sys.path.insert(0, ROOT)
     from oracle import oracle
     from specklesource_b200 import abi
     p = abi.TrackParams(nR=N_R, nA=nA, **dict(GRID, aStart=aStart))
     t = time.time()
-    o = oracle.strack(p, band1, band2, precision="f32")
-    return time.time() - t, nA * N_R, o["stats"]
+    o = oracle.strack(p, band1, band2, precision=precision)
+    return time.time() - t, nA * N_R, {k: o[k] for k in ("offR", "offA", "type")}
 
 
-def cpu_baseline(img1, img2, rows_per_worker=6, workers=None):
-    """The f32 oracle (reference-like precision) on rows_per_worker grid rows per
-    process, all host cores, spawned processes over disjoint azimuth bands."""
-    import multiprocessing as mp
-    workers = workers or os.cpu_count()
-    jobs = []
+def _row_jobs(img1, img2, rows_per_worker, workers, precision):
+    """One job per worker: rows_per_worker consecutive grid rows, the workers'
+    row blocks spread evenly over the grid, each with the image band covering
+    every window of its rows (large amplitude window and the secondary image's
+    shift included)."""
+    jobs, starts = [], []
     for w in range(workers):
-        i0 = w * rows_per_worker
-        # band covering every window of these rows (large amplitude window and
-        # the secondary image's shift included) with a margin
+        i0 = min(N_A - rows_per_worker, (w * N_A) // workers)
         a_lo = GRID["aStart"] + i0 * GRID["deltaA"] - W - 32
         a_hi = GRID["aStart"] + (i0 + rows_per_worker - 1) * GRID["deltaA"] + 2 * W + 32
         lo = max(0, a_lo)
         b1 = np.ascontiguousarray(img1[lo:a_hi])
         b2 = np.ascontiguousarray(img2[lo:a_hi])
         # aStart relative to the band keeps the window coordinates of the full grid
-        jobs.append((b1, b2, GRID["aStart"] + i0 * GRID["deltaA"] - lo, rows_per_worker))
+        jobs.append((b1, b2, GRID["aStart"] + i0 * GRID["deltaA"] - lo, rows_per_worker, precision))
+        starts.append(i0)
+    return jobs, starts
+
+
+def _run_pool(jobs):
+    import multiprocessing as mp
     ctx = mp.get_context("spawn")
     t0 = time.time()
-    with ctx.Pool(workers) as pool:
+    with ctx.Pool(len(jobs)) as pool:
         res = pool.map(_cpu_worker, jobs)
-    wall = time.time() - t0
+    return res, time.time() - t0
+
+
+def cpu_baseline(img1, img2, rows_per_worker=6, workers=None):
+    """The f32 oracle (reference-like precision) on rows_per_worker grid rows per
+    process, all host cores, spawned processes over azimuth bands spread over
+    the grid."""
+    workers = workers or os.cpu_count()
+    jobs, _ = _row_jobs(img1, img2, rows_per_worker, workers, "f32")
+    res, wall = _run_pool(jobs)
     pts = sum(r[1] for r in res)
     work = max(r[0] for r in res)
     return {"value": pts / work, "unit": "patches/s", "cores": workers, "kind": "port",
             "sample": f"{workers} processes x {rows_per_worker} grid rows x {N_R} patches ({pts} patches) of "
-                      f"the same workload, f32 CPU restatement (oracle/, gcc -O3), {work:.1f} s compute, "
-                      f"{wall:.1f} s wall incl. spawn"}
+                      f"the same workload spread over the grid, f32 CPU restatement (oracle/, gcc -O3), "
+                      f"{work:.1f} s compute, {wall:.1f} s wall incl. spawn"}
+
+
+def accuracy_vs_fp64(img1, img2, gpu, rows_per_worker=1, workers=None):
+    """Offsets of the GPU run against the FP64 oracle on a spread sample of grid
+    rows: error percentiles (px) on the points both match, the fraction within
+    0.02 px (0.01 px for complex matches), and match-type agreement."""
+    workers = workers or os.cpu_count()
+    jobs, starts = _row_jobs(img1, img2, rows_per_worker, workers, "f64")
+    res, wall = _run_pool(jobs)
+    errs, tol_ok, n_match, same, n_pts = [], 0, 0, 0, 0
+    for (_, _, o), i0 in zip(res, starts):
+        sl = slice(i0, i0 + rows_per_worker)
+        g = {k: gpu[k][sl] for k in ("offR", "offA", "type")}
+        matched = o["type"] > 0
+        both = matched & (g["type"] > 0)
+        e = np.maximum(np.abs(g["offR"].astype(np.float64) - o["offR"]),
+                       np.abs(g["offA"].astype(np.float64) - o["offA"]))
+        tol = np.where(o["type"] == 1, 0.01, 0.02)
+        tol_ok += int((both & (e <= tol)).sum())
+        n_match += int(matched.sum())
+        same += int((g["type"] == o["type"]).sum())
+        n_pts += o["type"].size
+        errs.append(e[both])
+    e = np.concatenate(errs) if errs else np.zeros(0)
+    return {"points": n_pts, "oracle_matches": n_match,
+            "frac_within_tol": tol_ok / max(1, n_match), "frac_same_type": same / max(1, n_pts),
+            "err_px_p50": float(np.percentile(e, 50)) if e.size else None,
+            "err_px_p99": float(np.percentile(e, 99)) if e.size else None,
+            "err_px_max": float(e.max()) if e.size else None,
+            "sample": f"{workers} x {rows_per_worker} grid rows spread over the grid, FP64 oracle, {wall:.1f} s"}
+
+
+def measured_traffic(kernel_key):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu
+    summary (a 'traffic_bytes_per_launch:' line), or None."""
+    path = os.path.join(ROOT, "profiles", f"{kernel_key}.md")
+    try:
+        with open(path) as f:
+            for ln in f:
+                if ln.startswith("traffic_bytes_per_launch:"):
+                    return int(ln.split(":")[1].strip())
+    except (OSError, ValueError):
+        return None
+    return None
 
 
 # ---------------------------------------------------------------- main
@@ -222,7 +285,7 @@ def run_reference(args):
             vals.append(r["value"])
             cb = r
     v = float(np.median(vals))
-    line = {"impl": "reference", "metric": "patches/s (strack, 64x64 windows, 12000x24000 pair)", "value": v,
+    line = {"impl": "reference", "metric": METRIC, "value": v,
             "unit": "patches/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * N_A * N_R / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded speckle pair, no public dataset)",
@@ -244,6 +307,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp32-peak", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the FP64-oracle check of a row sample")
     ap.add_argument("--workload", default="large", choices=["large", "small"],
                     help="small: 2400x4800 profiling case of the same generator")
     args = ap.parse_args()
@@ -285,10 +349,11 @@ def main():
     barrier()
     clocks = ClockSampler(local)
     clocks.start()
-    tot_ms, stages, launches = 0.0, [], 0
+    tot_ms, stages, launches, step_ms = 0.0, [], 0, []
     for _ in range(args.steps):
         t, st, nl = step_dev()
         tot_ms += t
+        step_ms.append(t)
         stages.append(st)
         launches += nl
     barrier()
@@ -334,15 +399,21 @@ def main():
                "d2h_bytes_per_step": n_pts * (4 * 4 + 1), "ms_per_step": e_ms,
                "match_fraction": float((hout["type"] > 0).mean())}
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    cpu, acc = None, None
+    if rank == 0 and world == 1 and not (args.no_cpu_baseline and args.no_accuracy):
         a = synth.to_numpy(s1)
         b = synth.to_numpy(s2)
-        cpu = cpu_baseline(a, b, rows_per_worker=args.cpu_rows)
+        if not args.no_cpu_baseline:
+            cpu = cpu_baseline(a, b, rows_per_worker=args.cpu_rows)
+        if not args.no_accuracy:
+            g = {k: out[k].cpu().numpy() for k in ("offR", "offA", "type")}
+            acc = accuracy_vs_fp64(a, b, g)
+    key = f"strack_cmplx_w64_{NA}x{NR}"
+    traffic = measured_traffic(key)
 
     if rank == 0:
         line = {
-            "metric": "patches/s (strack, 64x64 windows, 12000x24000 pair)",
+            "metric": METRIC,
             "value": value, "unit": "patches/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded speckle pair, no public dataset)",
@@ -350,11 +421,18 @@ def main():
                                    "fallback)", "parallelism": f"replicas x{world}",
                        "l2": "inputs 4.6 GB >> 126 MB L2, no flush"},
             "e2e": e2e,
+            "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
+                           "what": "one sb_strack call over the whole grid, images resident"},
+            "accuracy": acc,
             "gpu_launches": launches,
             "stages": {k: float(np.mean([s[k] for s in stages])) for k in stages[-1]},
             "roofline": {
                 "bound": "fp32", "achieved": ach_tflops, "peak": fp32, "unit": "TFLOP/s",
-                "frac": ach_tflops / fp32, "traffic": None,
+                "frac": ach_tflops / fp32,
+                "traffic": traffic,
+                "traffic_source": f"ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, profiles/{key}.md"
+                                  if traffic else "no committed capture for this workload",
+                "alg_bytes_per_launch": img_bytes + n_pts * (4 * 4 + 1),
                 "kernel": "strack_cmplx_kernel<64,512>",
                 "alg_flops_per_patch": ALG_CMPLX,
                 "peak_source": "cuBLAS SGEMM 8192^3 (TF32 off) measured in this run",
