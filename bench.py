@@ -297,6 +297,163 @@ def run_reference(args):
     return 0
 
 
+# ---------------------------------------------------------------- other configurations
+# Optional measurement modes for the benchmark's other configurations (not the
+# default bench line): cfg1 (1024 x 2048, W=32, complex + amplitude fallback and
+# amplitude only), cfg3 (strackw, 8000 x 16000 shear pair, search window 224,
+# edge pad 48, step 32, 5 x 5 box smoothing) and cull (the cullst passes on an
+# offsets grid of the default workload's size with 8 % outliers, 2 % NaN).
+
+def _band_worker(args):
+    fn, band1, band2, grid, precision = args
+    sys.path.insert(0, ROOT)
+    from oracle import oracle
+    from specklesource_b200 import abi
+    p = abi.TrackParams(**grid)
+    t = time.time()
+    o = getattr(oracle, fn)(p, band1, band2, precision=precision)
+    return time.time() - t, grid["nA"] * grid["nR"], {k: o[k] for k in ("offR", "offA", "type")}
+
+
+def _oracle_bands(fn, img1, img2, grid, row_blocks, margin, precision):
+    """Oracle over blocks (i0, nrows, r0, ncols) of a grid, one spawned process
+    per block, each given only the image band its windows reach."""
+    import multiprocessing as mp
+    jobs = []
+    for i0, nrows, j0, ncols in row_blocks:
+        a_lo = grid["aStart"] + i0 * grid["deltaA"] - margin
+        a_hi = grid["aStart"] + (i0 + nrows - 1) * grid["deltaA"] + margin
+        lo = max(0, a_lo)
+        g = dict(grid, nA=nrows, nR=ncols, aStart=grid["aStart"] + i0 * grid["deltaA"] - lo,
+                 rStart=grid["rStart"] + j0 * grid["deltaR"])
+        jobs.append((fn, np.ascontiguousarray(img1[lo:a_hi]), np.ascontiguousarray(img2[lo:a_hi]), g, precision))
+    ctx = mp.get_context("spawn")
+    t0 = time.time()
+    with ctx.Pool(len(jobs)) as pool:
+        res = pool.map(_band_worker, jobs)
+    return res, time.time() - t0
+
+
+def _accuracy(res, blocks, gpu):
+    errs, ok, n_match, same, n_pts = [], 0, 0, 0, 0
+    for (_, _, o), (i0, nrows, j0, ncols) in zip(res, blocks):
+        g = {k: gpu[k][i0:i0 + nrows, j0:j0 + ncols] for k in ("offR", "offA", "type")}
+        matched = o["type"] > 0
+        both = matched & (g["type"] > 0)
+        e = np.maximum(np.abs(g["offR"].astype(np.float64) - o["offR"]),
+                       np.abs(g["offA"].astype(np.float64) - o["offA"]))
+        tol = np.where(o["type"] == 1, 0.01, 0.02)
+        ok += int((both & (e <= tol)).sum())
+        n_match += int(matched.sum())
+        same += int((g["type"] == o["type"]).sum())
+        n_pts += o["type"].size
+        errs.append(e[both])
+    e = np.concatenate(errs) if errs else np.zeros(0)
+    pct = (lambda q: float(np.percentile(e, q)) if e.size else None)
+    return {"points": n_pts, "oracle_matches": n_match, "frac_within_tol": ok / max(1, n_match),
+            "frac_same_type": same / max(1, n_pts), "err_px_p50": pct(50), "err_px_p99": pct(99),
+            "err_px_max": float(e.max()) if e.size else None}
+
+
+def _time_calls(ctx, call, steps, warmup):
+    for _ in range(warmup):
+        call()
+    ms = []
+    for _ in range(steps):
+        call()
+        ms.append(ctx.timing()["total"])
+    return ms
+
+
+def run_other(args):
+    import torch
+    from specklesource_b200 import abi, runtime, synth
+    torch.cuda.set_device(0)
+    ctx = runtime.Context(0)
+    cores = os.cpu_count()
+    clocks = ClockSampler(0)
+    lines = []
+    if args.workload == "cfg1":
+        s1, s2 = synth.small_pair(device="cuda", na=1024, nr=2048)
+        a, b = synth.to_numpy(s1), synth.to_numpy(s2)
+        grid = dict(rStart=40, aStart=40, deltaR=16, deltaA=8, nR=124, nA=119, wR=32, wA=32, wRa=32, wAa=32)
+        for variant, extra in (("complex + amplitude fallback", {}), ("amplitude only (-noComplex)",
+                                                                     {"noComplex": 1})):
+            g = dict(grid, **extra)
+            p = abi.TrackParams(**g)
+            clocks = ClockSampler(0)
+            clocks.start()
+            ms = _time_calls(ctx, lambda: ctx.strack(p, s1, s2), args.steps, args.warmup)
+            clk = clocks.stop()
+            st = ctx.stage_timing()
+            res = ctx.strack(p, a, b)
+            n = grid["nR"] * grid["nA"]
+            rows = (grid["nA"] + cores - 1) // cores
+            blocks = [(i0, min(rows, grid["nA"] - i0), 0, grid["nR"]) for i0 in range(0, grid["nA"], rows)]
+            r32, w32 = _oracle_bands("strack", a, b, g, blocks, 2 * 32 + 48, "f32")
+            r64, _ = _oracle_bands("strack", a, b, g, blocks, 2 * 32 + 48, "f64")
+            cpu = n / max(r[0] for r in r32)
+            lines.append({"workload": f"cfg1 strack 1024x2048 w32 step 16x8, {variant}", "patches": n,
+                          "value": n / (np.median(ms) * 1e-3), "unit": "patches/s",
+                          "latency_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99))},
+                          "stages": st, "accuracy": _accuracy(r64, blocks, res),
+                          "cpu_baseline": {"value": cpu, "unit": "patches/s", "cores": len(blocks), "kind": "port",
+                                           "sample": "whole grid, f32 CPU restatement"},
+                          "clocks": clk})
+    elif args.workload in ("cfg3", "cfg3small"):
+        na, nr = (8000, 16000) if args.workload == "cfg3" else (2000, 4000)
+        s1, s2 = synth.shear_pair(device="cuda", na=na, nr=nr, seed=3)
+        Wn = 224
+        grid = dict(rStart=160, aStart=160, deltaR=32, deltaA=32, nR=(nr - 320) // 32 + 1, nA=(na - 320) // 32 + 1,
+                    wR=Wn, wA=Wn, wRa=Wn, wAa=Wn, edgePadR=48, edgePadA=48, navgR=2, navgA=2)
+        p = abi.TrackParams(**grid)
+        clocks.start()
+        ms = _time_calls(ctx, lambda: ctx.strackw(p, s1, s2), args.steps, args.warmup)
+        clk = clocks.stop()
+        res = ctx.strackw(p, s1, s2)
+        res = {k: (v.cpu().numpy() if hasattr(v, "cpu") else v) for k, v in res.items()}
+        a, b = synth.to_numpy(s1), synth.to_numpy(s2)
+        n = grid["nR"] * grid["nA"]
+        # one grid row segment of 12 points per core, spread over the grid
+        blocks = [((k * grid["nA"]) // cores, 1, (k * 37) % (grid["nR"] - 12), 12) for k in range(cores)]
+        r32, _ = _oracle_bands("strackw", a, b, grid, blocks, Wn, "f32")
+        r64, _ = _oracle_bands("strackw", a, b, grid, blocks, Wn, "f64")
+        cpu = sum(r[1] for r in r32) / max(r[0] for r in r32)
+        lines.append({"workload": f"cfg3 strackw {na}x{nr} shear, search 224, edge pad 48, step 32, navg 2",
+                      "patches": n, "value": n / (np.median(ms) * 1e-3), "unit": "patches/s",
+                      "latency_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99))},
+                      "accuracy": _accuracy(r64, blocks, res),
+                      "cpu_baseline": {"value": cpu, "unit": "patches/s", "cores": cores, "kind": "port",
+                                       "sample": f"{cores} x 12 points spread over the grid, f32 CPU restatement"},
+                      "clocks": clk})
+    elif args.workload == "cull":
+        from oracle import oracle
+        nA, nR = N_A, N_R
+        offR, offA, corr, mt = synth.offsets_field(nA, nR, 4)
+        cp = abi.CullParams(nR=nR, nA=nA, bR=5, bA=5, nGood=12, sR=3, sA=3, islandThresh=10, nCullPasses=3)
+        clocks.start()
+        ms = _time_calls(ctx, lambda: ctx.cull(cp, offR, offA, corr, mt), args.steps, args.warmup)
+        clk = clocks.stop()
+        g = ctx.cull(cp, offR, offA, corr, mt)
+        t = time.time()
+        o = oracle.cull(cp, offR, offA, corr, mt)
+        cpu_s = time.time() - t
+        keep = {k: bool(np.array_equal(g[k], o[k], equal_nan=True)) for k in ("offR", "offA", "type")}
+        lines.append({"workload": f"cull {nA}x{nR} grid, 8% outliers, 2% NaN, box 5, 3 passes, smooth 3x3, "
+                                  "islands 10", "points": nA * nR,
+                      "value": nA * nR / (np.median(ms) * 1e-3), "unit": "grid points/s",
+                      "latency_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99))},
+                      "keep_mask_bit_exact": keep,
+                      "cpu_baseline": {"value": nA * nR / cpu_s, "unit": "grid points/s", "cores": 1,
+                                       "kind": "port", "sample": "whole grid, FP64 CPU restatement"},
+                      "clocks": clk})
+    for ln in lines:
+        print(json.dumps(dict(ln, n_gpus=1, steps=args.steps, warmup=args.warmup, dtype="f32",
+                              data="synthetic (seeded)")))
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -308,11 +465,15 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp32-peak", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the FP64-oracle check of a row sample")
-    ap.add_argument("--workload", default="large", choices=["large", "small"],
-                    help="small: 2400x4800 profiling case of the same generator")
+    ap.add_argument("--workload", default="large", choices=["large", "small", "cfg1", "cfg3", "cfg3small", "cull"],
+                    help="small: 2400x4800 profiling case of the same generator; cfg1 / cfg3 / cull: the "
+                         "other configurations (one JSON line each, not the bench line); cfg3small: the cfg3 "
+                         "geometry on a 2000x4000 pair (profiling case)")
     args = ap.parse_args()
     if args.workload == "small":
         use_small_workload()
+    if args.workload in ("cfg1", "cfg3", "cfg3small", "cull"):
+        return run_other(args)
     if args.impl == "reference":
         return run_reference(args)
 

@@ -414,14 +414,91 @@ __device__ __forceinline__ void fft2d_smem(float2* base, const float2* __restric
     fft_lines<N1, N2, DIR, N * NIMG, N, NT, 1, RS, IS>(base, tw);  // columns: line = column
 }
 
-// 2-D transform of an N x N row-major array anywhere in memory (row stride N;
-// normally a per-CTA global workspace that stays in L2), staged through a
-// shared tile of G lines of N+1 float2: rows first, then columns.
-template <int N, int DIR, int NT>
-__device__ __forceinline__ void fft2d_staged(float2* g, float2* tile, const float2* __restrict__ tw)
+// ---------------------------------------------------------------- three-step lines
+// Large lengths N = N1 N2 N3 (x index n = M n1 + N3 n2 + n3 with M = N2 N3,
+// X index k = k1 + N1 k2 + N1 N2 k3): step A radix-N1 over n1 with twiddle
+// W_N^{k1 m}; step B radix-N2 over n2 inside each block of M with twiddle
+// W_N^{N1 k2 n3}; step C radix-N3 over the contiguous n3, handed to
+// out(l, k, value).  A and B are in place in `base`; C reads `base` and must
+// write elsewhere (out may not alias base), so nothing is held across a
+// barrier and every step needs at most max(N1, N2, N3) complex registers.
+template <int N> struct Split3;
+template <> struct Split3<32>  { static constexpr int N1 = 2, N2 = 4, N3 = 4; };
+template <> struct Split3<48>  { static constexpr int N1 = 3, N2 = 4, N3 = 4; };
+template <> struct Split3<64>  { static constexpr int N1 = 4, N2 = 4, N3 = 4; };
+template <> struct Split3<96>  { static constexpr int N1 = 6, N2 = 4, N3 = 4; };
+template <> struct Split3<128> { static constexpr int N1 = 8, N2 = 4, N3 = 4; };
+template <> struct Split3<192> { static constexpr int N1 = 3, N2 = 8, N3 = 8; };
+template <> struct Split3<224> { static constexpr int N1 = 7, N2 = 4, N3 = 8; };
+template <> struct Split3<256> { static constexpr int N1 = 4, N2 = 8, N3 = 8; };
+template <> struct Split3<384> { static constexpr int N1 = 6, N2 = 8, N3 = 8; };
+template <> struct Split3<448> { static constexpr int N1 = 7, N2 = 8, N3 = 8; };
+template <> struct Split3<512> { static constexpr int N1 = 8, N2 = 8, N3 = 8; };
+
+template <int N1, int N2, int N3, int DIR, int NL, int NT, int LS, int ES, typename Out>
+__device__ __forceinline__ void fft_lines3(float2* base, Out out, const float2* __restrict__ tw)
 {
-    constexpr int G = (N % 16 == 0) ? 16 : 8;
-    constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
+    constexpr int N = N1 * N2 * N3, M = N2 * N3;
+    const int tid = threadIdx.x;
+    for (int t = tid; t < NL * M; t += NT) {
+        const int l = t % NL, m = t / NL;
+        float2* p = base + l * LS + m * ES;
+        float2 v[N1];
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1) v[n1] = p[(M * n1) * ES];
+        RegDFT<N1, DIR, N>::run(v, tw);
+#pragma unroll
+        for (int k1 = 1; k1 < N1; ++k1) v[k1] = twmul_rt<DIR>(v[k1], tw, k1 * m);
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) p[(M * k1) * ES] = v[k1];
+    }
+    __syncthreads();
+    for (int t = tid; t < NL * N1 * N3; t += NT) {
+        const int l = t % NL, r = t / NL;
+        const int n3 = r % N3, k1 = r / N3;
+        float2* p = base + l * LS + (M * k1 + n3) * ES;
+        float2 v[N2];
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) v[n2] = p[(N3 * n2) * ES];
+        RegDFT<N2, DIR, N>::run(v, tw);
+#pragma unroll
+        for (int k2 = 1; k2 < N2; ++k2) v[k2] = twmul_rt<DIR>(v[k2], tw, N1 * k2 * n3);
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) p[(N3 * k2) * ES] = v[k2];
+    }
+    __syncthreads();
+    for (int t = tid; t < NL * N1 * N2; t += NT) {
+        const int l = t % NL, r = t / NL;
+        const int k2 = r % N2, k1 = r / N2;
+        const float2* p = base + l * LS + (M * k1 + N3 * k2) * ES;
+        float2 v[N3];
+#pragma unroll
+        for (int n3 = 0; n3 < N3; ++n3) v[n3] = p[n3 * ES];
+        RegDFT<N3, DIR, N>::run(v, tw);
+#pragma unroll
+        for (int k3 = 0; k3 < N3; ++k3) out(l, k1 + N1 * k2 + N1 * N2 * k3, v[k3]);
+    }
+    __syncthreads();
+}
+
+// 2-D transform of an N x N row-major array anywhere in memory (row stride N;
+// normally a per-CTA global workspace) staged through shared-memory tiles of
+// G lines: rows first, then columns.  THREE selects the three-step line form
+// (Split3<N>; fewest registers, G = 8 lines per tile), which writes its last
+// step out of place into `tileB`; the two-step form (Split<N>) works in place
+// and takes tileB = nullptr.  Tile sizes: StagedTile<N, THREE>.
+template <int N, bool THREE>
+struct StagedTile {
+    static constexpr int G = THREE ? 8 : ((N % 16 == 0) ? 16 : 8);
+    static constexpr int elems = (G * (N + 1) > N * (G + 1)) ? G * (N + 1) : N * (G + 1);
+    static constexpr int elemsB = THREE ? elems : 0;
+};
+
+template <int N, int DIR, int NT, bool THREE = false>
+__device__ __forceinline__ void fft2d_staged(float2* g, float2* tile, const float2* __restrict__ tw,
+                                             float2* tileB)
+{
+    constexpr int G = StagedTile<N, THREE>::G;
     const int tid = threadIdx.x;
     for (int r0 = 0; r0 < N; r0 += G) {
         for (int e = tid; e < G * N; e += NT) {
@@ -429,10 +506,21 @@ __device__ __forceinline__ void fft2d_staged(float2* g, float2* tile, const floa
             tile[l * (N + 1) + k] = g[(size_t)(r0 + l) * N + k];
         }
         __syncthreads();
-        fft_lines<N1, N2, DIR, G, G, NT, N + 1, 1, 0>(tile, tw);
-        for (int e = tid; e < G * N; e += NT) {
-            const int l = e / N, k = e % N;
-            g[(size_t)(r0 + l) * N + k] = tile[l * (N + 1) + k];
+        if constexpr (THREE) {
+            constexpr int N1 = Split3<N>::N1, N2 = Split3<N>::N2, N3 = Split3<N>::N3;
+            auto out = [tileB](int l, int k, float2 v) { tileB[l * (N + 1) + k] = v; };
+            fft_lines3<N1, N2, N3, DIR, G, NT, N + 1, 1>(tile, out, tw);
+            for (int e = tid; e < G * N; e += NT) {
+                const int l = e / N, k = e % N;
+                g[(size_t)(r0 + l) * N + k] = tileB[l * (N + 1) + k];
+            }
+        } else {
+            constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
+            fft_lines<N1, N2, DIR, G, G, NT, N + 1, 1, 0>(tile, tw);
+            for (int e = tid; e < G * N; e += NT) {
+                const int l = e / N, k = e % N;
+                g[(size_t)(r0 + l) * N + k] = tile[l * (N + 1) + k];
+            }
         }
         __syncthreads();
     }
@@ -442,19 +530,24 @@ __device__ __forceinline__ void fft2d_staged(float2* g, float2* tile, const floa
             tile[k * (G + 1) + l] = g[(size_t)k * N + c0 + l];
         }
         __syncthreads();
-        fft_lines<N1, N2, DIR, G, G, NT, 1, G + 1, 0>(tile, tw);
-        for (int e = tid; e < N * G; e += NT) {
-            const int k = e / G, l = e % G;
-            g[(size_t)k * N + c0 + l] = tile[k * (G + 1) + l];
+        if constexpr (THREE) {
+            constexpr int N1 = Split3<N>::N1, N2 = Split3<N>::N2, N3 = Split3<N>::N3;
+            auto out = [tileB](int l, int k, float2 v) { tileB[k * (G + 1) + l] = v; };
+            fft_lines3<N1, N2, N3, DIR, G, NT, 1, G + 1>(tile, out, tw);
+            for (int e = tid; e < N * G; e += NT) {
+                const int k = e / G, l = e % G;
+                g[(size_t)k * N + c0 + l] = tileB[k * (G + 1) + l];
+            }
+        } else {
+            constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
+            fft_lines<N1, N2, DIR, G, G, NT, 1, G + 1, 0>(tile, tw);
+            for (int e = tid; e < N * G; e += NT) {
+                const int k = e / G, l = e % G;
+                g[(size_t)k * N + c0 + l] = tile[k * (G + 1) + l];
+            }
         }
         __syncthreads();
     }
 }
-
-template <int N>
-struct StagedTile {
-    static constexpr int G = (N % 16 == 0) ? 16 : 8;
-    static constexpr int elems = (G * (N + 1) > N * (G + 1)) ? G * (N + 1) : N * (G + 1);
-};
 
 }  // namespace sbfft

@@ -25,9 +25,9 @@ template <int WS>
 struct NoallocCfg {
     static constexpr int N = 2 * WS;
     static constexpr int NT = 256;
-    static constexpr int TILE = sbfft::StagedTile<N>::elems > sbfft::StagedTile<WS>::elems
-                                    ? sbfft::StagedTile<N>::elems
-                                    : sbfft::StagedTile<WS>::elems;
+    static constexpr int TILE = sbfft::StagedTile<N, false>::elems > sbfft::StagedTile<WS, false>::elems
+                                    ? sbfft::StagedTile<N, false>::elems
+                                    : sbfft::StagedTile<WS, false>::elems;
     static constexpr size_t smem = sizeof(float2) * (TILE + WS + N + WS + OSW * NFAST + NFAST * OSW) +
                                    sizeof(float) * NFAST * NFAST + sizeof(double) * (NT / 32 + 1) * 8 +
                                    sizeof(int) * (3 * (NT / 32) + 8) + 64;
@@ -134,8 +134,8 @@ __global__ void __launch_bounds__(NoallocCfg<WS>::NT) amp_noalloc_kernel(Noalloc
             if (az < 0 || az >= WS) az = 0;
         }
         __syncthreads();
-        sbfft::fft2d_staged<WS, -1, NT>(F1, tile, twWs);
-        sbfft::fft2d_staged<WS, -1, NT>(F2, tile, twWs);
+        sbfft::fft2d_staged<WS, -1, NT>(F1, tile, twWs, nullptr);
+        sbfft::fft2d_staged<WS, -1, NT>(F2, tile, twWs, nullptr);
 #pragma unroll 1
         for (int q = 0; q < 2; ++q) {
             const float2* F = q == 0 ? F1 : F2;
@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(NoallocCfg<WS>::NT) amp_noalloc_kernel(Noalloc
                     work[e] = v;
                 }
                 __syncthreads();
-                sbfft::fft2d_staged<WS, 1, NT>(work, tile, twWs);
+                sbfft::fft2d_staged<WS, 1, NT>(work, tile, twWs, nullptr);
                 for (int e = tid; e < WS * WS; e += NT) {
                     const int m1 = e / WS, m2 = e % WS;
                     const float2 w = work[e];
@@ -201,7 +201,7 @@ __global__ void __launch_bounds__(NoallocCfg<WS>::NT) amp_noalloc_kernel(Noalloc
         }
         block_allsum<2, NT>(pw, red);
         const double p1 = pw[0] / nn, p2 = pw[1] / nn;
-        sbfft::fft2d_staged<N, -1, NT>(z, tile, twN);
+        sbfft::fft2d_staged<N, -1, NT>(z, tile, twN, nullptr);
         for (int e = tid; e < N * N; e += NT) {
             const int k1 = e / N, k2 = e % N;
             const int e2 = ((N - k1) % N) * N + ((N - k2) % N);
@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(NoallocCfg<WS>::NT) amp_noalloc_kernel(Noalloc
             z[e2] = make_float2(s.x, -s.y);
         }
         __syncthreads();
-        sbfft::fft2d_staged<N, 1, NT>(z, tile, twN);
+        sbfft::fft2d_staged<N, 1, NT>(z, tile, twN, nullptr);
         ArgMax best;
         best.v = 0.f;
         best.rank = 0x7fffffff;

@@ -26,9 +26,9 @@ template <int WS>
 struct AmpCfg {
     static constexpr int N = 2 * WS;
     static constexpr int NT = 256;
-    static constexpr int TILE = sbfft::StagedTile<N>::elems > sbfft::StagedTile<WS>::elems
-                                    ? sbfft::StagedTile<N>::elems
-                                    : sbfft::StagedTile<WS>::elems;
+    static constexpr int TILE = sbfft::StagedTile<N, false>::elems > sbfft::StagedTile<WS, false>::elems
+                                    ? sbfft::StagedTile<N, false>::elems
+                                    : sbfft::StagedTile<WS, false>::elems;
     static constexpr size_t smem = sizeof(float2) * (TILE + WS + N + WS + OSW * NFAST + NFAST * OSW) +
                                    sizeof(float) * NFAST * NFAST + sizeof(double) * (NT / 32 + 1) * 8 +
                                    sizeof(int) * (3 * (NT / 32) + 8) + 64;
@@ -117,8 +117,8 @@ __global__ void __launch_bounds__(AmpCfg<WS>::NT) strack_amp_kernel(AmpArgs a)
             if (azShift < 0) azShift = 0;
         }
         __syncthreads();
-        sbfft::fft2d_staged<WS, -1, NT>(F1, tile, twWs);
-        sbfft::fft2d_staged<WS, -1, NT>(F2, tile, twWs);
+        sbfft::fft2d_staged<WS, -1, NT>(F1, tile, twWs, nullptr);
+        sbfft::fft2d_staged<WS, -1, NT>(F2, tile, twWs, nullptr);
         const int az = (int)((float)azShift * (float)WS / (float)a.wA);
         // ---------------------------------------------------- detected images
 #pragma unroll 1
@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(AmpCfg<WS>::NT) strack_amp_kernel(AmpArgs a)
                     work[e] = v;
                 }
                 __syncthreads();
-                sbfft::fft2d_staged<WS, 1, NT>(work, tile, twWs);
+                sbfft::fft2d_staged<WS, 1, NT>(work, tile, twWs, nullptr);
                 for (int e = tid; e < WS * WS; e += NT) {
                     const int m1 = e / WS, m2 = e % WS;
                     const float2 w = work[e];
@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(AmpCfg<WS>::NT) strack_amp_kernel(AmpArgs a)
         block_allsum<2, NT>(pw, red);
         const double p1 = pw[0] / nn, p2 = pw[1] / nn;
         // ---------------------------------------------------- correlation
-        sbfft::fft2d_staged<N, -1, NT>(z, tile, twN);
+        sbfft::fft2d_staged<N, -1, NT>(z, tile, twN, nullptr);
         for (int e = tid; e < N * N; e += NT) {
             const int k1 = e / N, k2 = e % N;
             const int e2 = ((N - k1) % N) * N + ((N - k2) % N);
@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(AmpCfg<WS>::NT) strack_amp_kernel(AmpArgs a)
             z[e2] = make_float2(s.x, -s.y);
         }
         __syncthreads();
-        sbfft::fft2d_staged<N, 1, NT>(z, tile, twN);
+        sbfft::fft2d_staged<N, 1, NT>(z, tile, twN, nullptr);
         ArgMax best;
         best.v = 0.f;
         best.rank = 0x7fffffff;

@@ -110,30 +110,33 @@ template <int W>
 struct SwCfg {
     static constexpr int N = 2 * W;
     static constexpr int NT = 256;
-    static constexpr int TILE = sbfft::StagedTile<N>::elems > sbfft::StagedTile<W>::elems
-                                    ? sbfft::StagedTile<N>::elems
-                                    : sbfft::StagedTile<W>::elems;
-    static constexpr size_t smem = sizeof(float2) * (TILE + W + N + W) + sizeof(double) * (W_OSW * W_N1) +
+    static constexpr int TILE = sbfft::StagedTile<N, true>::elems > sbfft::StagedTile<W, true>::elems
+                                    ? sbfft::StagedTile<N, true>::elems
+                                    : sbfft::StagedTile<W, true>::elems;
+    static constexpr int TILEB = TILE;  // out-of-place tile of the three-step transforms
+    static constexpr size_t smem = sizeof(float2) * (TILE + TILEB + W + N + W) + sizeof(double) * (W_OSW * W_N1) +
                                    sizeof(double) * (W_N1 * W_N1 + W_N1 * W_OSW) + sizeof(double) * (NT / 32 + 1) * 8 +
                                    sizeof(int) * (3 * (NT / 32) + 8) + 64;
     static_assert((NT / 32) * 2 * N <= W * W, "per-warp prefix slices must fit in `work`");
     // workspace (float2 units): F1, F2, work (W^2 each), I1, I2 (N^2 floats
     // each), z (N^2), row sums RS1, RS2 (N x L doubles each), meanS, sigmaS,
-    // ncc (L^2 doubles each) with L = 4E + 1
+    // ncc (L^2 doubles each) with L = 4E + 1, then H1, H2 (N^2 floats each)
     static size_t perCta(int L)
     {
-        return (size_t)3 * W * W + (size_t)N * N + (size_t)N * N + (size_t)2 * N * L + (size_t)3 * L * L + 64;
+        return (size_t)3 * W * W + (size_t)N * N + (size_t)N * N + (size_t)2 * N * L + (size_t)3 * L * L +
+               (size_t)N * N + 64;
     }
 };
 
 template <int W>
-__global__ void __launch_bounds__(SwCfg<W>::NT) strackw_kernel(SwArgs a)
+__global__ void __launch_bounds__(SwCfg<W>::NT, 2) strackw_kernel(SwArgs a)
 {
     using C = SwCfg<W>;
     constexpr int N = C::N, NT = C::NT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2* tile = reinterpret_cast<float2*>(smem_raw);
-    float2* twW = tile + C::TILE;
+    float2* tileB = tile + C::TILE;
+    float2* twW = tileB + C::TILEB;
     float2* twN = twW + W;
     float2* tau = twN + N;
     double* Bm = reinterpret_cast<double*>(tau + W);      // 64 x 21
@@ -173,6 +176,8 @@ __global__ void __launch_bounds__(SwCfg<W>::NT) strackw_kernel(SwArgs a)
     double* meanS = RS2 + (size_t)N * L;
     double* sigmaS = meanS + (size_t)LA * L;
     double* ncc = sigmaS + (size_t)LA * L;
+    float* H1 = reinterpret_cast<float*>(ncc + (size_t)LA * L);
+    float* H2 = H1 + (size_t)N * N;
     const bool smooth = a.navgA > 1 || a.navgR > 1;
 
     for (int it = blockIdx.x; it < a.nList; it += gridDim.x) {
@@ -208,8 +213,8 @@ __global__ void __launch_bounds__(SwCfg<W>::NT) strackw_kernel(SwArgs a)
         }
         int da = (int)m[0];
         if (da < 0 || da >= W) da = 0;
-        sbfft::fft2d_staged<W, -1, NT>(F1, tile, twW);
-        sbfft::fft2d_staged<W, -1, NT>(F2, tile, twW);
+        sbfft::fft2d_staged<W, -1, NT, true>(F1, tile, twW, tileB);
+        sbfft::fft2d_staged<W, -1, NT, true>(F2, tile, twW, tileB);
         // ------------------------------------------------ upsampled intensities
 #pragma unroll 1
         for (int q = 0; q < 2; ++q) {
@@ -226,7 +231,7 @@ __global__ void __launch_bounds__(SwCfg<W>::NT) strackw_kernel(SwArgs a)
                     work[e] = v;
                 }
                 __syncthreads();
-                sbfft::fft2d_staged<W, 1, NT>(work, tile, twW);
+                sbfft::fft2d_staged<W, 1, NT, true>(work, tile, twW, tileB);
                 for (int e = tid; e < W * W; e += NT) {
                     const int m1 = e / W, m2 = e % W;
                     const float2 w = work[e];
@@ -236,6 +241,29 @@ __global__ void __launch_bounds__(SwCfg<W>::NT) strackw_kernel(SwArgs a)
             }
         }
         // ------------------------------------------------ detectPatch
+        // The (2 navg + 1)^2 box sums are separable: range sums into H1/H2
+        // first, then azimuth sums of those, with the reference's clamps
+        // (image 1: the N x N area; the chip: kmax/lmax, the azimuth limit
+        // built from edgePadR as at :795).
+        const int kmax = eR * OS + wA2 + a.navgA - 1;
+        const int lmax = eR * OS + wR2 + a.navgR - 1;
+        if (smooth) {
+            for (int e = tid; e < N * N; e += NT) {
+                const int i = e / N, j = e % N;
+                float h1 = 0.f, h2 = 0.f;
+                for (int nn = -a.navgR; nn <= a.navgR; nn++) {
+                    int l = j + nn;
+                    l = l > 0 ? l : 0;
+                    const int l1 = l < N - 1 ? l : N - 1;
+                    const int l2 = l < lmax ? l : lmax;
+                    h1 += I1[(size_t)i * N + l1];
+                    h2 += I2[(size_t)i * N + l2];
+                }
+                H1[e] = h1;
+                H2[e] = h2;
+            }
+            __syncthreads();
+        }
         double cs[3] = {0, 0, 0};
         for (int e = tid; e < N * N; e += NT) {
             const int i = e / N, j = e % N;
@@ -247,12 +275,7 @@ __global__ void __launch_bounds__(SwCfg<W>::NT) strackw_kernel(SwArgs a)
                     int k = i + mm;
                     k = k > 0 ? k : 0;
                     k = k < N - 1 ? k : N - 1;
-                    for (int nn = -a.navgR; nn <= a.navgR; nn++) {
-                        int l = j + nn;
-                        l = l > 0 ? l : 0;
-                        l = l < N - 1 ? l : N - 1;
-                        acc += I1[(size_t)k * N + l];
-                    }
+                    acc += H1[(size_t)k * N + j];
                 }
                 v1 = acc;
             } else {
@@ -264,18 +287,11 @@ __global__ void __launch_bounds__(SwCfg<W>::NT) strackw_kernel(SwArgs a)
             if (ci >= 0 && ci < wA2 && cj >= 0 && cj < wR2) {
                 if (smooth) {
                     float acc = 0.f;
-                    const int kmax = eR * OS + wA2 + a.navgA - 1;  // edgePadR in the azimuth clamp (:795)
-                    const int lmax = eR * OS + wR2 + a.navgR - 1;
                     for (int mm = -a.navgA; mm <= a.navgA; mm++) {
                         int k = i + mm;
                         k = k > 0 ? k : 0;
                         k = k < kmax ? k : kmax;
-                        for (int nn = -a.navgR; nn <= a.navgR; nn++) {
-                            int l = j + nn;
-                            l = l > 0 ? l : 0;
-                            l = l < lmax ? l : lmax;
-                            acc += I2[(size_t)k * N + l];
-                        }
+                        acc += H2[(size_t)k * N + j];
                     }
                     v2 = acc;
                 } else {
@@ -334,14 +350,40 @@ __global__ void __launch_bounds__(SwCfg<W>::NT) strackw_kernel(SwArgs a)
             }
             __syncthreads();
         }
-        // column sums over wA2 rows for every placement
+        // column prefix sums of the row-window sums (one thread per lag column;
+        // rows unrolled so the loads run ahead of the dependent adds), then the
+        // wA2-row window of every placement as a difference of two prefixes
+        for (int s1 = tid; s1 < L; s1 += NT) {
+            double c1 = 0.0, c2 = 0.0;
+            int l = 0;
+            for (; l + 8 <= N; l += 8) {
+                double v1[8], v2[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    v1[u] = RS1[(size_t)(l + u) * L + s1];
+                    v2[u] = RS2[(size_t)(l + u) * L + s1];
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    c1 += v1[u];
+                    c2 += v2[u];
+                    RS1[(size_t)(l + u) * L + s1] = c1;
+                    RS2[(size_t)(l + u) * L + s1] = c2;
+                }
+            }
+            for (; l < N; ++l) {
+                c1 += RS1[(size_t)l * L + s1];
+                c2 += RS2[(size_t)l * L + s1];
+                RS1[(size_t)l * L + s1] = c1;
+                RS2[(size_t)l * L + s1] = c2;
+            }
+        }
+        __syncthreads();
         for (int e = tid; e < LA * L; e += NT) {
             const int l1 = e / L, s1 = e % L;
-            double a1 = 0, a2 = 0;
-            for (int l = l1; l < l1 + wA2; ++l) {
-                a1 += RS1[(size_t)l * L + s1];
-                a2 += RS2[(size_t)l * L + s1];
-            }
+            const size_t hi = (size_t)(l1 + wA2 - 1) * L + s1, lo = (size_t)(l1 - 1) * L + s1;
+            const double a1 = RS1[hi] - (l1 > 0 ? RS1[lo] : 0.0);
+            const double a2 = RS2[hi] - (l1 > 0 ? RS2[lo] : 0.0);
             const double ms = a1 / nchip;
             meanS[e] = ms;
             sigmaS[e] = a2 / (double)(wR2 * wA2 - 1) - ms * ms;
@@ -369,7 +411,7 @@ __global__ void __launch_bounds__(SwCfg<W>::NT) strackw_kernel(SwArgs a)
             }
             __syncthreads();
         }
-        sbfft::fft2d_staged<N, -1, NT>(z, tile, twN);
+        sbfft::fft2d_staged<N, -1, NT, true>(z, tile, twN, tileB);
         for (int e = tid; e < N * N; e += NT) {
             const int k1 = e / N, k2 = e % N;
             const int e2 = ((N - k1) % N) * N + ((N - k2) % N);
@@ -382,7 +424,7 @@ __global__ void __launch_bounds__(SwCfg<W>::NT) strackw_kernel(SwArgs a)
             z[e2] = make_float2(s.x, -s.y);
         }
         __syncthreads();
-        sbfft::fft2d_staged<N, 1, NT>(z, tile, twN);
+        sbfft::fft2d_staged<N, 1, NT, true>(z, tile, twN, tileB);
         // ------------------------------------------------ getPeakCorr
         const double wR2p = W - 2 * eR, wA2p = W - 2 * eA;
         const double scaleW = 1.0 / ((OS * OS * OS * OS) * W * wA2p * W * wR2p);

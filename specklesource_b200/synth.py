@@ -141,3 +141,39 @@ def to_numpy(t):
 def to_big_endian(a):
     """complex64 array -> big-endian '>c8' array (the on-disk SLC format)."""
     return np.ascontiguousarray(a).astype(">c8")
+
+
+_LARGE = np.float32(-2e9)
+
+
+def offsets_field(nA, nR, seed, outliers=0.08, holes=0.02):
+    """Smooth offsets with uniform +-20 px outliers, NaN holes and failed points."""
+    rng = np.random.default_rng(seed)
+    yy, xx = np.mgrid[0:nA, 0:nR].astype(np.float64)
+    offR = 3 + 2 * np.sin(xx / 37.0) * np.cos(yy / 23.0) + 0.05 * rng.standard_normal((nA, nR))
+    offA = -1 + np.cos((xx + yy) / 41.0) + 0.05 * rng.standard_normal((nA, nR))
+    m = rng.random((nA, nR)) < outliers
+    offR[m] += rng.uniform(-20, 20, m.sum())
+    offA[m] += rng.uniform(-20, 20, m.sum())
+    h = rng.random((nA, nR)) < holes
+    offR[h] = np.nan
+    offA[h] = np.nan
+    f = rng.random((nA, nR)) < 0.05
+    offR[f] = _LARGE
+    offA[f] = _LARGE
+    # a failed region holding small valid islands (they survive the median
+    # passes and are removed by the island pass) and one larger valid patch
+    a0, r0 = nA // 5, nR // 5
+    block = (slice(a0, a0 + 60), slice(r0, r0 + 90))
+    offR[block] = _LARGE
+    offA[block] = _LARGE
+    f[block] = True
+    for k, (di, dj, s) in enumerate([(5, 5, 8), (5, 40, 7), (30, 10, 9), (30, 50, 25)]):
+        isl = (slice(a0 + di, a0 + di + s), slice(r0 + dj, r0 + dj + min(s, 35)))
+        offR[isl] = 3.0 + 0.01 * k
+        offA[isl] = -1.0
+        f[isl] = False
+    corr = rng.uniform(0, 1, (nA, nR)).astype(np.float32)
+    mt = rng.integers(1, 4, (nA, nR)).astype(np.uint8)
+    mt[f] = 0
+    return offR.astype(np.float32), offA.astype(np.float32), corr, mt
