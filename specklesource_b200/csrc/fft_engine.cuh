@@ -494,60 +494,86 @@ struct StagedTile {
     static constexpr int elemsB = THREE ? elems : 0;
 };
 
-template <int N, int DIR, int NT, bool THREE = false>
-__device__ __forceinline__ void fft2d_staged(float2* g, float2* tile, const float2* __restrict__ tw,
-                                             float2* tileB)
+// Line transforms of one staged tile (rows: G lines of N at stride N+1;
+// columns: lines at stride 1, elements at stride G+1).  Returns the tile
+// holding the result (tile, or tileB for the three-step form).
+template <int N, int DIR, int NT, bool THREE, int LS, int ES>
+__device__ __forceinline__ const float2* staged_tile_fft(float2* tile, float2* tileB, const float2* __restrict__ tw)
+{
+    constexpr int G = StagedTile<N, THREE>::G;
+    if constexpr (THREE) {
+        constexpr int N1 = Split3<N>::N1, N2 = Split3<N>::N2, N3 = Split3<N>::N3;
+        auto out = [tileB](int l, int k, float2 v) { tileB[l * LS + k * ES] = v; };
+        fft_lines3<N1, N2, N3, DIR, G, NT, LS, ES>(tile, out, tw);
+        return tileB;
+    } else {
+        constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
+        fft_lines<N1, N2, DIR, G, G, NT, LS, ES, 0>(tile, tw);
+        return tile;
+    }
+}
+
+// Row pass of a staged N x N transform: row r of gout becomes DFT_N(src(r, .)).
+// src(r, k) may read row r of gout itself (in place): a tile of G rows is
+// loaded completely before it is written back.
+template <int N, int DIR, int NT, bool THREE, typename Src>
+__device__ __forceinline__ void staged_rows(float2* gout, Src src, float2* tile, float2* tileB,
+                                            const float2* __restrict__ tw)
 {
     constexpr int G = StagedTile<N, THREE>::G;
     const int tid = threadIdx.x;
     for (int r0 = 0; r0 < N; r0 += G) {
+#pragma unroll 4
         for (int e = tid; e < G * N; e += NT) {
             const int l = e / N, k = e % N;
-            tile[l * (N + 1) + k] = g[(size_t)(r0 + l) * N + k];
+            tile[l * (N + 1) + k] = src(r0 + l, k);
         }
         __syncthreads();
-        if constexpr (THREE) {
-            constexpr int N1 = Split3<N>::N1, N2 = Split3<N>::N2, N3 = Split3<N>::N3;
-            auto out = [tileB](int l, int k, float2 v) { tileB[l * (N + 1) + k] = v; };
-            fft_lines3<N1, N2, N3, DIR, G, NT, N + 1, 1>(tile, out, tw);
-            for (int e = tid; e < G * N; e += NT) {
-                const int l = e / N, k = e % N;
-                g[(size_t)(r0 + l) * N + k] = tileB[l * (N + 1) + k];
-            }
-        } else {
-            constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
-            fft_lines<N1, N2, DIR, G, G, NT, N + 1, 1, 0>(tile, tw);
-            for (int e = tid; e < G * N; e += NT) {
-                const int l = e / N, k = e % N;
-                g[(size_t)(r0 + l) * N + k] = tile[l * (N + 1) + k];
-            }
+        const float2* res = staged_tile_fft<N, DIR, NT, THREE, N + 1, 1>(tile, tileB, tw);
+#pragma unroll 4
+        for (int e = tid; e < G * N; e += NT) {
+            const int l = e / N, k = e % N;
+            gout[(size_t)(r0 + l) * N + k] = res[l * (N + 1) + k];
         }
         __syncthreads();
     }
+}
+
+// Column pass of a staged N x N transform: column c becomes DFT_N(src(., c)),
+// handed element by element to dst(k, c, value).
+template <int N, int DIR, int NT, bool THREE, typename Src, typename Dst>
+__device__ __forceinline__ void staged_cols(Src src, Dst dst, float2* tile, float2* tileB,
+                                            const float2* __restrict__ tw)
+{
+    constexpr int G = StagedTile<N, THREE>::G;
+    const int tid = threadIdx.x;
     for (int c0 = 0; c0 < N; c0 += G) {
+#pragma unroll 4
         for (int e = tid; e < N * G; e += NT) {
             const int k = e / G, l = e % G;
-            tile[k * (G + 1) + l] = g[(size_t)k * N + c0 + l];
+            tile[k * (G + 1) + l] = src(k, c0 + l);
         }
         __syncthreads();
-        if constexpr (THREE) {
-            constexpr int N1 = Split3<N>::N1, N2 = Split3<N>::N2, N3 = Split3<N>::N3;
-            auto out = [tileB](int l, int k, float2 v) { tileB[k * (G + 1) + l] = v; };
-            fft_lines3<N1, N2, N3, DIR, G, NT, 1, G + 1>(tile, out, tw);
-            for (int e = tid; e < N * G; e += NT) {
-                const int k = e / G, l = e % G;
-                g[(size_t)k * N + c0 + l] = tileB[k * (G + 1) + l];
-            }
-        } else {
-            constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
-            fft_lines<N1, N2, DIR, G, G, NT, 1, G + 1, 0>(tile, tw);
-            for (int e = tid; e < N * G; e += NT) {
-                const int k = e / G, l = e % G;
-                g[(size_t)k * N + c0 + l] = tile[k * (G + 1) + l];
-            }
+        const float2* res = staged_tile_fft<N, DIR, NT, THREE, 1, G + 1>(tile, tileB, tw);
+#pragma unroll 4
+        for (int e = tid; e < N * G; e += NT) {
+            const int k = e / G, l = e % G;
+            dst(k, c0 + l, res[k * (G + 1) + l]);
         }
         __syncthreads();
     }
+}
+
+// 2-D transform of an N x N row-major array anywhere in memory (row stride N;
+// normally a per-CTA global workspace) staged through the tiles: rows, then
+// columns, in place.
+template <int N, int DIR, int NT, bool THREE = false>
+__device__ __forceinline__ void fft2d_staged(float2* g, float2* tile, const float2* __restrict__ tw,
+                                             float2* tileB)
+{
+    staged_rows<N, DIR, NT, THREE>(g, [g](int r, int k) { return g[(size_t)r * N + k]; }, tile, tileB, tw);
+    staged_cols<N, DIR, NT, THREE>([g](int k, int c) { return g[(size_t)k * N + c]; },
+                                   [g](int k, int c, float2 v) { g[(size_t)k * N + c] = v; }, tile, tileB, tw);
 }
 
 }  // namespace sbfft

@@ -216,28 +216,36 @@ __global__ void __launch_bounds__(SwCfg<W>::NT, 2) strackw_kernel(SwArgs a)
         sbfft::fft2d_staged<W, -1, NT, true>(F1, tile, twW, tileB);
         sbfft::fft2d_staged<W, -1, NT, true>(F2, tile, twW, tileB);
         // ------------------------------------------------ upsampled intensities
+        // The 2W x 2W padded inverse as four parity transforms
+        // c_e[m1][m2] = IDFT_W(X' tau_e1[k1] tau_e2[k2]), X'[k1] = F[(k1 + da) mod W]:
+        // the row factor tau_e1 and the row roll commute with the row
+        // transform, so two unrolled row passes (R0 = rows of F, R1 = rows of
+        // F tau) serve the four parities, and each column pass reads its R with
+        // the roll and tau_e1 folded into the gather and writes |c|^2 * scale
+        // straight into the intensity plane.
 #pragma unroll 1
         for (int q = 0; q < 2; ++q) {
-            const float2* F = q == 0 ? F1 : F2;
+            float2* F = q == 0 ? F1 : F2;
             float* I = q == 0 ? I1 : I2;
+            const float sc = a.scale;
+            sbfft::staged_rows<W, 1, NT, true>(
+                work, [F](int r, int k) { return F[(size_t)r * W + k]; }, tile, tileB, twW);
+            sbfft::staged_rows<W, 1, NT, true>(
+                F, [F, tau](int r, int k) { return sbfft::cmul(F[(size_t)r * W + k], tau[k]); }, tile, tileB, twW);
 #pragma unroll 1
             for (int par = 0; par < 4; ++par) {
                 const int e1 = par >> 1, e2 = par & 1;
-                for (int e = tid; e < W * W; e += NT) {
-                    const int k1 = e / W, k2 = e % W;
-                    float2 v = F[((k1 + da) % W) * W + k2];
-                    if (e1) v = sbfft::cmul(v, tau[k1]);
-                    if (e2) v = sbfft::cmul(v, tau[k2]);
-                    work[e] = v;
-                }
-                __syncthreads();
-                sbfft::fft2d_staged<W, 1, NT, true>(work, tile, twW, tileB);
-                for (int e = tid; e < W * W; e += NT) {
-                    const int m1 = e / W, m2 = e % W;
-                    const float2 w = work[e];
-                    I[(size_t)(2 * m1 + e1) * N + 2 * m2 + e2] = (w.x * w.x + w.y * w.y) * a.scale;
-                }
-                __syncthreads();
+                const float2* R = e2 ? F : work;
+                auto src = [R, tau, da, e1](int k, int c) {
+                    int r = k + da;
+                    r = r >= W ? r - W : r;
+                    const float2 v = R[(size_t)r * W + c];
+                    return e1 ? sbfft::cmul(v, tau[k]) : v;
+                };
+                auto dst = [I, sc, e1, e2](int k, int c, float2 v) {
+                    I[(size_t)(2 * k + e1) * N + 2 * c + e2] = (v.x * v.x + v.y * v.y) * sc;
+                };
+                sbfft::staged_cols<W, 1, NT, true>(src, dst, tile, tileB, twW);
             }
         }
         // ------------------------------------------------ detectPatch
