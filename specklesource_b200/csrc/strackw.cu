@@ -405,34 +405,46 @@ __global__ void __launch_bounds__(SwCfg<W>::NT, 2) strackw_kernel(SwArgs a)
         // difference directly, because sum(chip - meanR) = 0 over the support:
         //   sum_x (chip[x] - meanR)(A1[x+t] - mA1) = c[t] - meanR * n * meanS[t].
         // Same quantity, without the float cancellation.
+        // The mean removal is folded into the forward row pass; the Hermitian
+        // split of the packed pair and the cross spectrum into the inverse row
+        // pass, which reads Z[k] and Z[-k] and writes out of place into the
+        // free H1/H2 area (Zi); the last column pass keeps only the lag rows
+        // and columns getPeakCorr reads.
         {
             const float mA1 = (float)(cs[2] / ((double)N * N));
             const float mR = (float)meanR;
-            for (int e = tid; e < N * N; e += NT) {
-                const int i = e / N, j = e % N;
-                const int ci = i - eA * OS, cj = j - eR * OS;
+            const int cA = eA * OS, cR = eR * OS;
+            auto srcFwd = [z, mA1, mR, cA, cR, wA2, wR2](int r, int k) {
+                float2 v = z[(size_t)r * N + k];
+                const int ci = r - cA, cj = k - cR;
                 const bool in = ci >= 0 && ci < wA2 && cj >= 0 && cj < wR2;
-                float2 v = z[e];
                 v.x -= mA1;
                 v.y = in ? v.y - mR : 0.f;
-                z[e] = v;
-            }
-            __syncthreads();
+                return v;
+            };
+            sbfft::staged_rows<N, -1, NT, true>(z, srcFwd, tile, tileB, twN);
+            sbfft::staged_cols<N, -1, NT, true>([z](int k, int c) { return z[(size_t)k * N + c]; },
+                                                [z](int k, int c, float2 v) { z[(size_t)k * N + c] = v; }, tile,
+                                                tileB, twN);
         }
-        sbfft::fft2d_staged<N, -1, NT, true>(z, tile, twN, tileB);
-        for (int e = tid; e < N * N; e += NT) {
-            const int k1 = e / N, k2 = e % N;
-            const int e2 = ((N - k1) % N) * N + ((N - k2) % N);
-            if (e2 < e) continue;
-            const float2 Zk = z[e], Zm = z[e2];
-            const float2 f1 = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
-            const float2 f2 = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
-            const float2 s = sbfft::cconjmul(f1, f2);
-            z[e] = s;
-            z[e2] = make_float2(s.x, -s.y);
+        float2* Zi = reinterpret_cast<float2*>(H1);
+        {
+            auto srcInv = [z](int r, int k) {
+                const float2 Zk = z[(size_t)r * N + k];
+                const float2 Zm = z[(size_t)(r == 0 ? 0 : N - r) * N + (k == 0 ? 0 : N - k)];
+                const float2 f1 = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
+                const float2 f2 = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
+                return sbfft::cconjmul(f1, f2);
+            };
+            sbfft::staged_rows<N, 1, NT, true>(Zi, srcInv, tile, tileB, twN);
+            const int nLo = LA - OS * eA, nHi = N - OS * eA;  // lag rows/cols used: [0, nLo) and [nHi, N)
+            auto need = [nLo, nHi](int x) { return x < nLo || x >= nHi; };
+            sbfft::staged_cols<N, 1, NT, true>([Zi](int k, int c) { return Zi[(size_t)k * N + c]; },
+                                               [Zi, need](int k, int c, float2 v) {
+                                                   if (need(k) && need(c)) Zi[(size_t)k * N + c] = v;
+                                               },
+                                               tile, tileB, twN);
         }
-        __syncthreads();
-        sbfft::fft2d_staged<N, 1, NT, true>(z, tile, twN, tileB);
         // ------------------------------------------------ getPeakCorr
         const double wR2p = W - 2 * eR, wA2p = W - 2 * eA;
         const double scaleW = 1.0 / ((OS * OS * OS * OS) * W * wA2p * W * wR2p);
@@ -444,7 +456,7 @@ __global__ void __launch_bounds__(SwCfg<W>::NT, 2) strackw_kernel(SwArgs a)
             const int i = e / L, j = e % L;
             const int l = i - OS * eA, s = j - OS * eR;
             const int cy = l < 0 ? l + N : l, cx = s < 0 ? s + N : s;
-            const float2 c = z[(size_t)cy * N + cx];
+            const float2 c = Zi[(size_t)cy * N + cx];
             double v = (double)c.x * scaleW;  // = |c| * scaleW - meanR * meanS (the covariance)
             v = v / sqrt(sigmaR * sigmaS[e]);
             ncc[e] = v;
