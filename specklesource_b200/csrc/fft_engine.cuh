@@ -423,6 +423,8 @@ __device__ __forceinline__ void fft2d_smem(float2* base, const float2* __restric
 // write elsewhere (out may not alias base), so nothing is held across a
 // barrier and every step needs at most max(N1, N2, N3) complex registers.
 template <int N> struct Split3;
+template <> struct Split3<16>  { static constexpr int N1 = 2, N2 = 2, N3 = 4; };
+template <> struct Split3<24>  { static constexpr int N1 = 2, N2 = 3, N3 = 4; };
 template <> struct Split3<32>  { static constexpr int N1 = 2, N2 = 4, N3 = 4; };
 template <> struct Split3<48>  { static constexpr int N1 = 3, N2 = 4, N3 = 4; };
 template <> struct Split3<64>  { static constexpr int N1 = 4, N2 = 4, N3 = 4; };

@@ -26,10 +26,10 @@ template <int WS>
 struct AmpCfg {
     static constexpr int N = 2 * WS;
     static constexpr int NT = 256;
-    static constexpr int TILE = sbfft::StagedTile<N, false>::elems > sbfft::StagedTile<WS, false>::elems
-                                    ? sbfft::StagedTile<N, false>::elems
-                                    : sbfft::StagedTile<WS, false>::elems;
-    static constexpr size_t smem = sizeof(float2) * (TILE + WS + N + WS + OSW * NFAST + NFAST * OSW) +
+    static constexpr int TILE = sbfft::StagedTile<N, true>::elems > sbfft::StagedTile<WS, true>::elems
+                                    ? sbfft::StagedTile<N, true>::elems
+                                    : sbfft::StagedTile<WS, true>::elems;  // tile and the out-of-place tileB
+    static constexpr size_t smem = sizeof(float2) * (2 * TILE + WS + N + WS + OSW * NFAST + NFAST * OSW) +
                                    sizeof(float) * NFAST * NFAST + sizeof(double) * (NT / 32 + 1) * 8 +
                                    sizeof(int) * (3 * (NT / 32) + 8) + 64;
     // workspace: F1, F2, work (Ws^2 each), z (N^2), mag (N^2 floats)
@@ -37,13 +37,14 @@ struct AmpCfg {
 };
 
 template <int WS>
-__global__ void __launch_bounds__(AmpCfg<WS>::NT) strack_amp_kernel(AmpArgs a)
+__global__ void __launch_bounds__(AmpCfg<WS>::NT, 2) strack_amp_kernel(AmpArgs a)
 {
     using C = AmpCfg<WS>;
     constexpr int N = C::N, NT = C::NT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2* tile = reinterpret_cast<float2*>(smem_raw);
-    float2* twWs = tile + C::TILE;
+    float2* tileB = tile + C::TILE;
+    float2* twWs = tileB + C::TILE;
     float2* twN = twWs + WS;
     float2* tau = twN + N;
     float2* osA = tau + WS;
@@ -117,42 +118,57 @@ __global__ void __launch_bounds__(AmpCfg<WS>::NT) strack_amp_kernel(AmpArgs a)
             if (azShift < 0) azShift = 0;
         }
         __syncthreads();
-        sbfft::fft2d_staged<WS, -1, NT>(F1, tile, twWs, nullptr);
-        sbfft::fft2d_staged<WS, -1, NT>(F2, tile, twWs, nullptr);
+        sbfft::fft2d_staged<WS, -1, NT, true>(F1, tile, twWs, tileB);
+        sbfft::fft2d_staged<WS, -1, NT, true>(F2, tile, twWs, tileB);
         const int az = (int)((float)azShift * (float)WS / (float)a.wA);
         // ---------------------------------------------------- detected images
-#pragma unroll 1
-        for (int q = 0; q < 2; ++q) {
-            const float2* F = q == 0 ? F1 : F2;
-#pragma unroll 1
-            for (int par = 0; par < 4; ++par) {
-                const int e1 = par >> 1, e2 = par & 1;
-                for (int e = tid; e < WS * WS; e += NT) {
-                    const int k1 = e / WS, k2 = e % WS;
-                    float2 v = F[((k1 + az) % WS) * WS + k2];
-                    if (e1) v = sbfft::cmul(v, tau[k1]);
-                    if (e2) v = sbfft::cmul(v, tau[k2]);
-                    work[e] = v;
-                }
-                __syncthreads();
-                sbfft::fft2d_staged<WS, 1, NT>(work, tile, twWs, nullptr);
-                for (int e = tid; e < WS * WS; e += NT) {
-                    const int m1 = e / WS, m2 = e % WS;
-                    const float2 w = work[e];
-                    const float I = (w.x * w.x + w.y * w.y) * scale;
-                    float* zz = reinterpret_cast<float*>(&z[(size_t)(2 * m1 + e1) * N + 2 * m2 + e2]);
-                    zz[q] = I;
-                }
-                __syncthreads();
-            }
-        }
-        // ---------------------------------------------------- tests, amplitude, mean removal
+        // Four parity transforms per image as two row passes (rows of F and of
+        // F tau; the Doppler roll and tau_e1 commute with the row transform)
+        // and four column passes that fold the roll and tau_e1 into their
+        // gather and write |c|^2 * scale into component q of z.  The second
+        // image's epilogue also counts the samples under the threshold in
+        // either image, and each accumulates its own intensity sum.
         double r3[3] = {0, 0, 0};
-        for (int e = tid; e < N * N; e += NT) {
-            const float2 v = z[e];
-            if (v.x < thr || v.y < thr) r3[0] += 1.0;
-            r3[1] += v.x;
-            r3[2] += v.y;
+        {
+            float* zf = reinterpret_cast<float*>(z);
+            float cnt = 0.f;
+            double s1 = 0.0, s2 = 0.0;
+#pragma unroll 1
+            for (int q = 0; q < 2; ++q) {
+                float2* F = q == 0 ? F1 : F2;
+                sbfft::staged_rows<WS, 1, NT, true>(
+                    work, [F](int r, int k) { return F[(size_t)r * WS + k]; }, tile, tileB, twWs);
+                sbfft::staged_rows<WS, 1, NT, true>(
+                    F, [F, tau](int r, int k) { return sbfft::cmul(F[(size_t)r * WS + k], tau[k]); }, tile, tileB,
+                    twWs);
+#pragma unroll 1
+                for (int par = 0; par < 4; ++par) {
+                    const int e1 = par >> 1, e2 = par & 1;
+                    const float2* R = e2 ? F : work;
+                    auto src = [R, tau, az, e1](int k, int c) {
+                        int r = k + az;
+                        r = r >= WS ? r - WS : r;
+                        const float2 v = R[(size_t)r * WS + c];
+                        return e1 ? sbfft::cmul(v, tau[k]) : v;
+                    };
+                    auto dst = [zf, scale, e1, e2, q, thr, &cnt, &s1, &s2](int k, int c, float2 v) {
+                        const float I = (v.x * v.x + v.y * v.y) * scale;
+                        const size_t o = 2 * ((size_t)(2 * k + e1) * N + 2 * c + e2);
+                        if (q == 0) {
+                            zf[o] = I;
+                            s1 += I;
+                        } else {
+                            zf[o + 1] = I;
+                            s2 += I;
+                            cnt += (zf[o] < thr || I < thr) ? 1.f : 0.f;
+                        }
+                    };
+                    sbfft::staged_cols<WS, 1, NT, true>(src, dst, tile, tileB, twWs);
+                }
+            }
+            r3[0] = cnt;
+            r3[1] = s1;
+            r3[2] = s2;
         }
         block_allsum<3, NT>(r3, red);
         const bool hd = !(r3[0] > 20.0) && !(r3[1] < 1.0e-6 || r3[2] < 1.0e-6);
@@ -189,7 +205,7 @@ __global__ void __launch_bounds__(AmpCfg<WS>::NT) strack_amp_kernel(AmpArgs a)
         block_allsum<2, NT>(pw, red);
         const double p1 = pw[0] / nn, p2 = pw[1] / nn;
         // ---------------------------------------------------- correlation
-        sbfft::fft2d_staged<N, -1, NT>(z, tile, twN, nullptr);
+        sbfft::fft2d_staged<N, -1, NT, true>(z, tile, twN, tileB);
         for (int e = tid; e < N * N; e += NT) {
             const int k1 = e / N, k2 = e % N;
             const int e2 = ((N - k1) % N) * N + ((N - k2) % N);
@@ -203,7 +219,7 @@ __global__ void __launch_bounds__(AmpCfg<WS>::NT) strack_amp_kernel(AmpArgs a)
             z[e2] = make_float2(s.x, -s.y);
         }
         __syncthreads();
-        sbfft::fft2d_staged<N, 1, NT>(z, tile, twN, nullptr);
+        sbfft::fft2d_staged<N, 1, NT, true>(z, tile, twN, tileB);
         ArgMax best;
         best.v = 0.f;
         best.rank = 0x7fffffff;
