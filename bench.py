@@ -21,6 +21,7 @@ Under torchrun every rank tracks its own pair (weak scaling, no collective on
 the data path); rank 0 prints the max-over-ranks time.
 """
 import argparse
+import collections
 import json
 import os
 import subprocess
@@ -365,6 +366,151 @@ def _time_calls(ctx, call, steps, warmup):
     return ms
 
 
+def _plant_outliers(seed):
+    """Injects 8 % uniform +-20 px outliers and 2 % NaN holes into matched points."""
+    def inject(offR, offA, corr, mt):
+        rng = np.random.default_rng(seed)
+        ok = mt > 0
+        m = ok & (rng.random(offR.shape) < 0.08)
+        offR[m] += rng.uniform(-20, 20, m.sum()).astype(np.float32)
+        offA[m] += rng.uniform(-20, 20, m.sum()).astype(np.float32)
+        h = ok & (rng.random(offR.shape) < 0.02)
+        offR[h] = np.nan
+        offA[h] = np.nan
+    return inject
+
+
+def _tile_job(serve, abi, synth, torch, k, na, nr, w, radius, seed, cull=True, mode=None):
+    """One synthetic tile job.  w <= 64: strack with complex window w (amplitude
+    fallback on; mode "amplitude" runs -noComplex); w in (96, 128): strackw
+    with search window w + 2 radius rounded to a supported size and edge pad
+    radius.  Grid step w / 2, windows inside the tile."""
+    s1, s2 = synth.make_pair(na, nr, seed,
+                             dr=lambda y, x: 1.5 + 1.0 * torch.sin(2 * np.pi * x / 900),
+                             da=lambda y, x: 0.5 * torch.cos(2 * np.pi * y / 700),
+                             coherence=0.6, device="cuda")
+    if w <= 64:
+        W = w
+        margin = W + 8
+        step = max(8, W // 2)
+        nR, nA = (nr - 2 * margin) // step + 1, (na - 2 * margin) // step + 1
+        p = abi.TrackParams(rStart=margin, aStart=margin, deltaR=step, deltaA=step, nR=nR, nA=nA, wR=W, wA=W,
+                            wRa=W, wAa=W, noComplex=int(mode == "amplitude"))
+        kind = "strack"
+    else:
+        Ws = {96: 128, 128: 192}[w]
+        pad = min(max(radius, 8), Ws // 2 - 24)  # strackw needs edgepad >= NFAST/4 = 5
+        step = w // 2
+        margin = Ws // 2 + 8
+        nR, nA = (nr - 2 * margin) // step + 1, (na - 2 * margin) // step + 1
+        p = abi.TrackParams(rStart=margin, aStart=margin, deltaR=step, deltaA=step, nR=nR, nA=nA, wR=w, wA=w,
+                            wRa=Ws, wAa=Ws, edgePadR=pad, edgePadA=pad, navgR=2, navgA=2)
+        kind = "strackw"
+    if nR < 1 or nA < 1:
+        return None
+    cp = abi.CullParams(nR=nR, nA=nA, bR=5, bA=5, nGood=12, sR=3, sA=3, islandThresh=10) if cull else None
+    return serve.Job(kind=kind, params=p, img1=s1, img2=s2, cull=cp, inject=_plant_outliers(seed) if cull else None,
+                     tag=k)
+
+
+def run_batched(args):
+    """cfg4: 256 tiles (sides U[512, 4096], seeded) mixing windows
+    {24, 32, 48, 64, 96, 128} and radii {4, 8, 16, 32}, all submitted at once
+    to the job server; every offsets grid then goes through cullst (box 5,
+    3 passes, 3x3 smoothing, islands 10) with 8 % outliers and 2 % NaN planted."""
+    import torch
+    from specklesource_b200 import abi, serve, synth
+    rng = np.random.default_rng(4)
+    jobs = []
+    for k in range(256):
+        na, nr = (int(x) for x in rng.integers(512, 4097, 2))
+        w = int(rng.choice([24, 32, 48, 64, 96, 128]))
+        radius = int(rng.choice([4, 8, 16, 32]))
+        j = _tile_job(serve, abi, synth, torch, k, na, nr, w, radius, seed=400 + k)
+        if j is not None:
+            jobs.append(j)
+    torch.cuda.synchronize()
+    pts = sum(j.params.nR * j.params.nA for j in jobs)
+    clocks = ClockSampler(0)
+    with serve.JobServer(slots=args.slots, hbm_budget=120e9) as srv:
+        srv.submit(jobs[0]).result()  # warm-up: tables and buffers of one slot
+        clocks.start()
+        t0 = time.perf_counter()
+        for j in jobs:
+            j.arrival = 0.0
+        res = [f.result() for f in [srv.submit(j) for j in jobs]]
+        wall = time.perf_counter() - t0
+        clk = clocks.stop()
+    n_w = collections.Counter(("strack w%d" % j.params.wR) if j.kind == "strack" else
+                              ("strackw w%d" % j.params.wRa) for j in jobs)
+    matched = sum(int((r["track"]["type"] > 0).sum()) for r in res)
+    return {"workload": f"cfg4 {len(jobs)} tiles 512-4096 px, windows 24-128, strack/strackw + cullst, "
+                        f"{args.slots} server slots", "patches": pts, "value": pts / wall,
+            "unit": "patches/s (tracking + culling, wall clock)", "wall_s": wall,
+            "jobs_per_s": len(jobs) / wall, "matched_fraction": matched / pts, "mix": dict(n_w),
+            "note": "jobs overlap across server slots (one CUDA stream each); no single persistent launch",
+            "clocks": clk}
+
+
+def run_serving(args):
+    """cfg5: Poisson arrivals (40 jobs/s, seeded) of track + cull jobs on pairs
+    of 1024^2 - 8192^2 px (log-uniform), amplitude-only or complex mode,
+    window 32 - 64 (strack's complex window limit; search radius follows the
+    reference's acceptance rule |shift| < W/4), images resident in HBM,
+    admitted against a 120 GB budget.  Reports jobs/s, patches/s and the
+    arrival-to-completion latency percentiles."""
+    import torch
+    from specklesource_b200 import abi, serve, synth
+    rng = np.random.default_rng(5)
+    n_jobs = args.jobs
+    # a pool of resident pairs to crop from (generating 8192^2 pairs per job
+    # would time the generator, not the server)
+    pool = {}
+    for side in (1024, 2048, 4096, 8192):
+        pool[side] = synth.make_pair(side, side, 500 + side,
+                                     dr=lambda y, x: 1.5 + 1.0 * torch.sin(2 * np.pi * x / 900),
+                                     da=lambda y, x: 0.5 * torch.cos(2 * np.pi * y / 700),
+                                     coherence=0.6, device="cuda")
+    jobs = []
+    for k in range(n_jobs):
+        side = int(np.exp(rng.uniform(np.log(1024), np.log(8192))))
+        src = min(s for s in pool if s >= side)
+        a, b = pool[src]
+        mode = "amplitude" if rng.random() < 0.5 else "complex"
+        W = int(rng.choice([32, 48, 64]))
+        margin, step = W + 8, W // 2
+        n = (side - 2 * margin) // step + 1
+        p = abi.TrackParams(rStart=margin, aStart=margin, deltaR=step, deltaA=step, nR=n, nA=n, wR=W, wA=W, wRa=W,
+                            wAa=W, noComplex=int(mode == "amplitude"))
+        cp = abi.CullParams(nR=n, nA=n, bR=5, bA=5, nGood=12, sR=3, sA=3, islandThresh=10)
+        jobs.append((serve.Job(kind="strack", params=p, img1=a[:side, :side].contiguous(),
+                               img2=b[:side, :side].contiguous(), cull=cp, tag=k), side))
+    torch.cuda.synchronize()
+    gaps = rng.exponential(1.0 / 40.0, n_jobs)
+    clocks = ClockSampler(0)
+    with serve.JobServer(slots=args.slots, hbm_budget=120e9) as srv:
+        srv.submit(jobs[0][0]).result()
+        clocks.start()
+        t0 = time.perf_counter()
+        futs, t_next = [], t0
+        for (j, _), g in zip(jobs, gaps):
+            t_next += g
+            while time.perf_counter() < t_next:
+                time.sleep(min(0.002, max(0.0, t_next - time.perf_counter())))
+            j.arrival = time.perf_counter()
+            futs.append(srv.submit(j))
+        res = [f.result() for f in futs]
+        wall = max(r["end"] for r in res) - t0
+        clk = clocks.stop()
+        peak = srv.peak_bytes
+    pts = sum(j.params.nR * j.params.nA for j, _ in jobs)
+    return {"workload": f"cfg5 serving: {n_jobs} Poisson(40/s) track+cull jobs, 1024-8192 px, amplitude or "
+                        f"complex, W 32-64, {args.slots} slots, 120 GB budget", "jobs": n_jobs,
+            "value": n_jobs / wall, "unit": "jobs/s", "patches_per_s": pts / wall,
+            "latency_ms": serve.latency_stats(res), "offered_jobs_per_s": 40.0, "wall_s": wall,
+            "peak_admitted_gb": peak / 1e9, "clocks": clk}
+
+
 def run_other(args):
     import torch
     from specklesource_b200 import abi, runtime, synth
@@ -426,6 +572,8 @@ def run_other(args):
                       "cpu_baseline": {"value": cpu, "unit": "patches/s", "cores": cores, "kind": "port",
                                        "sample": f"{cores} x 12 points spread over the grid, f32 CPU restatement"},
                       "clocks": clk})
+    elif args.workload in ("cfg4", "cfg5"):
+        lines.append(run_batched(args) if args.workload == "cfg4" else run_serving(args))
     elif args.workload == "cull":
         from oracle import oracle
         nA, nR = N_A, N_R
@@ -465,14 +613,16 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp32-peak", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the FP64-oracle check of a row sample")
-    ap.add_argument("--workload", default="large", choices=["large", "small", "cfg1", "cfg3", "cfg3small", "cull"],
+    ap.add_argument("--slots", type=int, default=4, help="job-server slots for --workload cfg4/cfg5")
+    ap.add_argument("--jobs", type=int, default=200, help="jobs offered in --workload cfg5")
+    ap.add_argument("--workload", default="large", choices=["large", "small", "cfg1", "cfg3", "cfg3small", "cfg4", "cfg5", "cull"],
                     help="small: 2400x4800 profiling case of the same generator; cfg1 / cfg3 / cull: the "
                          "other configurations (one JSON line each, not the bench line); cfg3small: the cfg3 "
                          "geometry on a 2000x4000 pair (profiling case)")
     args = ap.parse_args()
     if args.workload == "small":
         use_small_workload()
-    if args.workload in ("cfg1", "cfg3", "cfg3small", "cull"):
+    if args.workload in ("cfg1", "cfg3", "cfg3small", "cfg4", "cfg5", "cull"):
         return run_other(args)
     if args.impl == "reference":
         return run_reference(args)

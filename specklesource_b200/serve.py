@@ -1,0 +1,207 @@
+"""Tracking-job server for one GPU: continuous batching of strack/strackw +
+cullst jobs.
+
+A job is one image pair tracked with `strack` (Strack/speckleTrack.c) or
+`strackw` (Strackw/corrTrackFast.c), optionally followed by the cullst passes
+(Cullst/cullst.c:71-101) on its offsets grid.  The server owns `slots` library
+contexts; each has its own CUDA stream and reusable device buffers and is
+driven by its own host thread, so jobs on different slots overlap on the GPU
+(the C calls release the GIL).  A job starts when a slot is free and its
+estimated device memory fits the HBM budget; admission is first come, first
+served (the head of the queue is never bypassed, so a large job cannot
+starve).  Images may be torch CUDA tensors (device-resident, nothing copied)
+or host arrays (copied inside the call).  Results are the same whether a job
+runs alone or beside others: every kernel is deterministic and contexts share
+no buffers.
+"""
+import collections
+import threading
+import time
+from concurrent.futures import Future
+from dataclasses import dataclass, field
+from typing import Any, Callable, Optional
+
+import numpy as np
+
+from . import abi
+
+# per-point device buffers of one strack call (plan, record, lists, fit job,
+# five output grids), bytes
+_STRACK_POINT_BYTES = 20 + 80 + 16 + 160 + 17 + 64
+# per-CTA workspaces (float2 elements), sized like the kernels' own
+_AMP_SCRATCH = {16: 3 * 16 * 16 + 32 * 32 * 3 // 2, 24: 3 * 24 * 24 + 48 * 48 * 3 // 2,
+                32: 3 * 32 * 32 + 64 * 64 * 3 // 2, 48: 3 * 48 * 48 + 96 * 96 * 3 // 2,
+                64: 3 * 64 * 64 + 128 * 128 * 3 // 2, 96: 3 * 96 * 96 + 192 * 192 * 3 // 2,
+                128: 3 * 128 * 128 + 256 * 256 * 3 // 2}
+
+
+@dataclass
+class Job:
+    """One tracking job.  kind: "strack" or "strackw"; cull: CullParams or
+    None; inject: optional callable(offR, offA, corr, type) run on the host
+    copies of the offsets before culling (used to plant outliers)."""
+    kind: str
+    params: Any
+    img1: Any
+    img2: Any
+    cull: Any = None
+    inject: Optional[Callable] = None
+    tag: Any = None
+    arrival: float = field(default=0.0)
+
+
+def _image_bytes(img):
+    try:
+        import torch
+        if isinstance(img, torch.Tensor):
+            return 0 if img.is_cuda else img.numel() * img.element_size()
+    except ImportError:
+        pass
+    return int(np.asarray(img).nbytes)
+
+
+def job_device_bytes(job, num_sm=148):
+    """Upper estimate of the device memory a job holds while it runs."""
+    p = job.params
+    n = int(p.nR) * int(p.nA)
+    b = _image_bytes(job.img1) + _image_bytes(job.img2)
+    ctas = 2 * num_sm
+    if job.kind == "strack":
+        b += n * _STRACK_POINT_BYTES
+        if p.maxTries > 0:
+            wa = int(p.wRa)
+            b += ctas * 8 * _AMP_SCRATCH.get(wa, _AMP_SCRATCH[128])
+            if p.maxTries > 1 and 2 * wa in _AMP_SCRATCH:
+                b += ctas * 8 * _AMP_SCRATCH[2 * wa]
+    else:
+        W = int(p.wRa)
+        N = 2 * W
+        L = 4 * (int(p.edgePadR) + 5) + 1
+        b += n * 40 + ctas * 8 * (3 * W * W + 3 * N * N + 2 * N * L + 3 * L * L)
+    if job.cull is not None:
+        b += n * 64
+    return int(b)
+
+
+class JobServer:
+    """Continuous-batching server.  context_factory(device) -> an object with
+    the runtime.Context methods strack/strackw/cull/close (a fake one in the
+    CPU tests)."""
+
+    def __init__(self, device=0, slots=4, hbm_budget=120e9, context_factory=None, num_sm=148):
+        if context_factory is None:
+            from . import runtime
+            context_factory = runtime.Context
+        self.budget = float(hbm_budget)
+        self.num_sm = num_sm
+        self._ctx = [context_factory(device) for _ in range(slots)]
+        self._cv = threading.Condition()
+        self._queue = collections.deque()
+        self._in_use = 0.0
+        self._peak = 0.0
+        self._closed = False
+        self.started = []  # (tag, start time) in admission order
+        self._threads = [threading.Thread(target=self._worker, args=(k,), daemon=True) for k in range(slots)]
+        for t in self._threads:
+            t.start()
+
+    @property
+    def peak_bytes(self):
+        return self._peak
+
+    def submit(self, job):
+        """Queues a job; returns a Future resolving to a dict with the track
+        result, the cull result (or None) and the job's start/end times."""
+        fut = Future()
+        need = job_device_bytes(job, self.num_sm)
+        if need > self.budget:
+            fut.set_exception(ValueError(f"job needs ~{need / 1e9:.1f} GB, above the {self.budget / 1e9:.1f} GB "
+                                         "HBM budget"))
+            return fut
+        job.arrival = job.arrival or time.perf_counter()
+        with self._cv:
+            if self._closed:
+                raise RuntimeError("server closed")
+            self._queue.append((job, need, fut))
+            self._cv.notify_all()
+        return fut
+
+    def _take(self):
+        with self._cv:
+            while True:
+                if self._closed and not self._queue:
+                    return None
+                if self._queue:
+                    job, need, fut = self._queue[0]
+                    if self._in_use + need <= self.budget:
+                        self._queue.popleft()
+                        self._in_use += need
+                        self._peak = max(self._peak, self._in_use)
+                        self.started.append((job.tag, time.perf_counter()))
+                        self._cv.notify_all()
+                        return job, need, fut
+                self._cv.wait()
+
+    def _release(self, need):
+        with self._cv:
+            self._in_use -= need
+            self._cv.notify_all()
+
+    def _worker(self, k):
+        ctx = self._ctx[k]
+        while True:
+            item = self._take()
+            if item is None:
+                return
+            job, need, fut = item
+            try:
+                t0 = time.perf_counter()
+                res = run_job(ctx, job)
+                res.update(start=t0, end=time.perf_counter(), arrival=job.arrival, slot=k)
+                fut.set_result(res)
+            except Exception as e:  # reported through the future
+                fut.set_exception(e)
+            finally:
+                self._release(need)
+
+    def close(self):
+        with self._cv:
+            self._closed = True
+            self._cv.notify_all()
+        for t in self._threads:
+            t.join()
+        for c in self._ctx:
+            c.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def run_job(ctx, job):
+    """Runs one job on a context (also how a job runs alone)."""
+    if job.kind == "strack":
+        tr = ctx.strack(job.params, job.img1, job.img2)
+    elif job.kind == "strackw":
+        tr = ctx.strackw(job.params, job.img1, job.img2)
+    else:
+        raise ValueError(f"unknown job kind {job.kind!r}")
+    cu = None
+    if job.cull is not None:
+        offR = np.array(tr["offR"], np.float32, copy=True)
+        offA = np.array(tr["offA"], np.float32, copy=True)
+        corr = np.array(tr["corr"], np.float32, copy=True)
+        mt = np.array(tr["type"], np.uint8, copy=True)
+        if job.inject is not None:
+            job.inject(offR, offA, corr, mt)
+        cu = ctx.cull(job.cull, offR, offA, corr, mt)
+    return {"track": tr, "cull": cu}
+
+
+def latency_stats(results):
+    """p50/p99 of arrival-to-completion latency (ms) over result dicts."""
+    lat = np.array([1e3 * (r["end"] - r["arrival"]) for r in results])
+    return {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+            "max": float(lat.max()), "mean": float(lat.mean())}

@@ -1,0 +1,123 @@
+"""The tracking-job server: admission against the HBM budget, FIFO order,
+errors through the futures (CPU, with a fake context), and -- on the GPU --
+identical results for jobs run alone and in a concurrent mix."""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+from specklesource_b200 import abi, serve
+
+
+class FakeContext:
+    """Stands in for runtime.Context: records concurrency, sleeps a little."""
+    lock = threading.Lock()
+    running = 0
+    max_running = 0
+
+    def __init__(self, device):
+        self.closed = False
+
+    def _run(self, p):
+        with FakeContext.lock:
+            FakeContext.running += 1
+            FakeContext.max_running = max(FakeContext.max_running, FakeContext.running)
+        time.sleep(0.02)
+        with FakeContext.lock:
+            FakeContext.running -= 1
+        if p.nR == 13:
+            raise RuntimeError("planted failure")
+        g = np.full((p.nA, p.nR), float(p.nR), np.float32)
+        return {"offR": g, "offA": g.copy(), "corr": g.copy(), "type": np.ones((p.nA, p.nR), np.uint8)}
+
+    def strack(self, p, a, b):
+        return self._run(p)
+
+    def strackw(self, p, a, b):
+        return self._run(p)
+
+    def cull(self, cp, offR, offA, corr, mt):
+        return {"offRS": offR + 1}
+
+    def close(self):
+        self.closed = True
+
+
+def _job(nR, nA=4, kind="strack", cull=False):
+    img = np.zeros((8, 8), np.complex64)
+    return serve.Job(kind=kind, params=abi.TrackParams(nR=nR, nA=nA), img1=img, img2=img,
+                     cull=abi.CullParams(nR=nR, nA=nA) if cull else None, tag=nR)
+
+
+def test_budget_limits_concurrency_and_order():
+    FakeContext.running = FakeContext.max_running = 0
+    one = serve.job_device_bytes(_job(10))
+    # room for two jobs at a time although four slots are free
+    with serve.JobServer(slots=4, hbm_budget=2.5 * one, context_factory=FakeContext) as srv:
+        futs = [srv.submit(_job(10 + (k % 2) * 0)) for k in range(8)]
+        res = [f.result(timeout=10) for f in futs]
+        assert srv.peak_bytes <= 2.5 * one
+    assert FakeContext.max_running == 2
+    assert all(r["track"]["offR"][0, 0] == 10 for r in res)
+    assert all(r["end"] >= r["start"] >= r["arrival"] for r in res)
+
+
+def test_fifo_admission_and_cull_and_errors():
+    FakeContext.running = FakeContext.max_running = 0
+    with serve.JobServer(slots=1, hbm_budget=1e12, context_factory=FakeContext) as srv:
+        jobs = [_job(nR, cull=True) for nR in (5, 6, 13, 7)]
+        futs = [srv.submit(j) for j in jobs]
+        assert futs[0].result(timeout=10)["cull"]["offRS"][0, 0] == 6
+        with pytest.raises(RuntimeError, match="planted"):
+            futs[2].result(timeout=10)
+        assert futs[3].result(timeout=10)["track"]["offR"][0, 0] == 7
+        assert [t for t, _ in srv.started] == [5, 6, 13, 7]
+
+
+def test_job_above_budget_is_refused():
+    with serve.JobServer(slots=1, hbm_budget=1000, context_factory=FakeContext) as srv:
+        f = srv.submit(_job(100, 100))
+        with pytest.raises(ValueError, match="HBM budget"):
+            f.result(timeout=5)
+
+
+def test_latency_stats():
+    rs = [{"arrival": 0.0, "end": 0.001 * k} for k in range(1, 101)]
+    st = serve.latency_stats(rs)
+    assert abs(st["p50"] - 50.5) < 1e-6 and st["max"] == 100.0
+
+
+@pytest.mark.gpu
+def test_same_result_alone_and_in_the_mix():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from specklesource_b200 import build, runtime, synth
+    build.build()
+    jobs = []
+    for k, (na, nr) in enumerate([(512, 768), (640, 1024), (512, 512), (768, 768), (600, 900), (512, 1024)]):
+        s1, s2 = synth.small_pair(device="cuda", na=na, nr=nr, seed=20 + k)
+        W = (32, 48, 64)[k % 3]
+        nRg, nAg = (nr - 2 * W) // (W // 2), (na - 2 * W) // (W // 2)
+        if k % 2 == 0:
+            p = abi.TrackParams(rStart=W, aStart=W, deltaR=W // 2, deltaA=W // 2, nR=nRg, nA=nAg, wR=W, wA=W,
+                                wRa=W, wAa=W, noComplex=k % 4 == 2)
+            kind = "strack"
+        else:
+            p = abi.TrackParams(rStart=2 * W, aStart=2 * W, deltaR=W // 2, deltaA=W // 2, nR=nRg - 4,
+                                nA=nAg - 4, wR=W, wA=W, wRa=2 * W, wAa=2 * W, edgePadR=8, edgePadA=8,
+                                navgR=2, navgA=2)
+            kind = "strackw"
+        jobs.append(serve.Job(kind=kind, params=p, img1=s1, img2=s2,
+                              cull=abi.CullParams(nR=p.nR, nA=p.nA, islandThresh=4), tag=k))
+    with runtime.Context(0) as ctx:
+        alone = [serve.run_job(ctx, j) for j in jobs]
+    with serve.JobServer(slots=3, hbm_budget=60e9) as srv:
+        mixed = [f.result(timeout=600) for f in [srv.submit(j) for j in jobs]]
+    assert len({r["slot"] for r in mixed}) > 1
+    for a, m in zip(alone, mixed):
+        for k in ("offR", "offA", "corr", "type"):
+            assert np.array_equal(a["track"][k], m["track"][k], equal_nan=True), k
+        for k in ("offRS", "offAS", "type"):
+            assert np.array_equal(a["cull"][k], m["cull"][k], equal_nan=True), k
