@@ -727,16 +727,26 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
         a.tw2Ws = tw_table(c, 2 * Ws);
         a.tau = tau_table(c, Ws);
         a.osA = osA_table(c);
+        a.osD = osD_table(c);
         a.rec = drec;
         a.fit = dfit;
-        int nCta = c->numSM * 2;
+        // small windows: everything in shared memory; larger: per-CTA
+        // workspace in global memory staged through shared tiles
+        const bool onChip = amps_supported(Ws);
+        int nCta = c->numSM * (onChip ? amps_blocks_per_sm(Ws) : 2);
         if (nCta > cnt) nCta = cnt;
-        a.scratchPerCta = amp_scratch_elems(Ws);
-        a.scratch = (float2*)sb_ctx_buf(c, "ampScratch", sizeof(float2) * a.scratchPerCta * nCta, &e);
-        if (!a.scratch || !a.twWs || !a.tw2Ws || !a.tau || !a.osA)
+        if (nCta < 1) return sb_ctx_fail(c, SB_ERR_CUDA, "amplitude kernel cannot be resident (Ws=%d)", Ws);
+        if (!onChip) {
+            a.scratchPerCta = amp_scratch_elems(Ws);
+            a.scratch = (float2*)sb_ctx_buf(c, "ampScratch", sizeof(float2) * a.scratchPerCta * nCta, &e);
+        }
+        if ((!onChip && !a.scratch) || !a.twWs || !a.tw2Ws || !a.tau || !a.osA || !a.osD)
             return sb_ctx_fail(c, SB_ERR_NOMEM, "amplitude workspace allocation failed");
         cudaEventRecord(c->sev[2 + 2 * stage], c->stream);
-        CK(launch_strack_amp(Ws, a, nCta, c->stream), "strack_amp");
+        if (onChip)
+            CK(launch_strack_amps(Ws, a, nCta, c->stream), "strack_amps");
+        else
+            CK(launch_strack_amp(Ws, a, nCta, c->stream), "strack_amp");
         c->launches++;
         cudaEventRecord(c->sev[3 + 2 * stage], c->stream);
         FitArgs f = make_fit_args(p, dfit, cnt, stage, drec);

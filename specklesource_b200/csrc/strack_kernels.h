@@ -56,6 +56,7 @@ struct AmpArgs {
     const float2* tw2Ws;  // W_{2Ws} table
     const float2* tau;    // parity twiddles for Ws
     const float2* osA;
+    const float2* osD;    // real form of the oversampling matrix (shared-memory kernel)
     float2* scratch;      // per-CTA workspace
     size_t scratchPerCta; // float2 elements
     PointRec* rec;
@@ -70,5 +71,10 @@ bool amp_supported(int Ws);
 size_t amp_scratch_elems(int Ws);
 int amp_threads(int Ws);
 cudaError_t launch_strack_amp(int Ws, const AmpArgs& a, int nCta, cudaStream_t st);
+
+// shared-memory-resident amplitude tries for small windows
+bool amps_supported(int Ws);
+int amps_blocks_per_sm(int Ws);
+cudaError_t launch_strack_amps(int Ws, const AmpArgs& a, int nCta, cudaStream_t st);
 
 }  // namespace sbk
