@@ -2,7 +2,9 @@
 //
 //  cullSTData (cullSTData.c:13-125): the median test runs in place in raster
 //    order, so a cull changes the neighbourhoods of later points.  The GPU
-//    keeps that order exactly with a row wavefront: one warp per grid row
+//    first solves that recurrence as a parallel fixpoint (cull_fix_kernel,
+//    exact when it converges); otherwise it keeps the order with a row
+//    wavefront: one warp per grid row
 //    (rows claimed in increasing order from a counter, so the row a warp waits
 //    on is always held by a running warp), each warp walks its row left to
 //    right and, before deciding column j, waits until the previous row has
@@ -207,6 +209,116 @@ __global__ void cull_median_kernel(CullArgs a, long long spinLimit)
         }
     }
     if (lane == 0 && culledHere) atomicAdd(a.nCulled, culledHere);
+}
+
+// ---------------------------------------------------------------- median pass, parallel fixpoint
+// The sequential pass decides point p from the values at the start of the pass
+// and from the decisions of the points before p (raster order) in its box:
+// C[p] = decide(p, {C[q] : q < p, q in box(p)}).  This recurrence over a DAG
+// has exactly one solution, the sequential result.  Jacobi iteration
+// C_{t+1} = decide(., C_t) from C_0 = 0 reaches it, and a step that changes
+// nothing proves it was reached (a fixpoint of the recurrence is its solution).
+// A point is recomputed only when a predecessor in its box changed in the
+// previous step.  offR/offA are not modified until the fixpoint is applied;
+// one warp per point, medians as in the wavefront kernel.
+struct FixArgs {
+    const float* offR;
+    const float* offA;
+    const uint8_t* cin;
+    uint8_t* cout;
+    const uint8_t* chgIn;  // null: first step, every point computed
+    uint8_t* chgOut;
+    int nR, nA, bR, bA, nGood;
+    float maxA, maxR;
+    unsigned int* nChanged;
+};
+
+template <int NV>
+__global__ void cull_fix_kernel(FixArgs a)
+{
+    const int lane = threadIdx.x & 31;
+    const int hA = a.bA / 2, hR = a.bR / 2;
+    const long long n = (long long)a.nR * a.nA;
+    const long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    unsigned int changedHere = 0;
+    for (long long p = w0; p < n; p += nw) {
+        const int i = (int)(p / a.nR), j = (int)(p % a.nR);
+        const int i1 = i - hA > 0 ? i - hA : 0, i2 = i + hA < a.nA - 1 ? i + hA : a.nA - 1;
+        const int j1 = j - hR > 0 ? j - hR : 0, j2 = j + hR < a.nR - 1 ? j + hR : a.nR - 1;
+        const int cols = j2 - j1 + 1, cnt = (i2 - i1 + 1) * cols;
+        if (a.chgIn) {
+            bool any = false;
+            for (int e = lane; e < cnt; e += 32) {
+                const long long q = (long long)(i1 + e / cols) * a.nR + (j1 + e % cols);
+                any |= q < p && a.chgIn[q];
+            }
+            if (!__any_sync(0xffffffffu, any)) {
+                if (lane == 0) {
+                    a.cout[p] = a.cin[p];
+                    a.chgOut[p] = 0;
+                }
+                continue;
+            }
+        }
+        uint32_t kr[NV], ka[NV];
+        uint32_t vm = 0;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            const int e = lane + 32 * v;
+            kr[v] = ka[v] = 0;
+            if (e < cnt) {
+                const long long q = (long long)(i1 + e / cols) * a.nR + (j1 + e % cols);
+                const float r = a.offR[q], az = a.offA[q];
+                if (valid_pt(r, az) && !(q < p && a.cin[q])) {
+                    vm |= 1u << v;
+                    kr[v] = fkey(r);
+                    ka[v] = fkey(az);
+                }
+            }
+        }
+        int ngood = 0;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) ngood += (vm >> v) & 1u;
+        ngood = __reduce_add_sync(0xffffffffu, ngood);
+        bool cull;
+        if ((unsigned)ngood > (unsigned)a.nGood) {
+            int mid = ngood / 2;
+            if (mid < 1) mid = 1;
+            const float medR = fkey_inv(warp_kth<NV>(kr, vm, mid));
+            const float medA = fkey_inv(warp_kth<NV>(ka, vm, mid));
+            const float oR = a.offR[p], oA = a.offA[p];
+            const double dA = (double)(oA - medA), dR = (double)(oR - medR);
+            cull = fabs(dA) > a.maxA || fabs(dR) > a.maxR;
+        } else {
+            cull = true;
+        }
+        if (lane == 0) {
+            const uint8_t c = cull ? 1 : 0;
+            a.cout[p] = c;
+            const uint8_t ch = c != a.cin[p];
+            a.chgOut[p] = ch;
+            changedHere += ch;
+        }
+    }
+    if (lane == 0 && changedHere) atomicAdd(a.nChanged, changedHere);
+}
+
+// Writes the culls of the converged pass; counts them.
+__global__ void cull_apply_kernel(float* offR, float* offA, const uint8_t* c, long long n,
+                                  unsigned long long* nCulled)
+{
+    unsigned long long k = 0;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+         p += (long long)gridDim.x * blockDim.x) {
+        if (c[p]) {
+            offR[p] = kCulled;
+            offA[p] = kCulled;
+            k++;
+        }
+    }
+    k = __reduce_add_sync(0xffffffffu, (unsigned)k);
+    if ((threadIdx.x & 31) == 0 && k) atomicAdd(nCulled, k);
 }
 
 // ---------------------------------------------------------------- stats
@@ -608,6 +720,67 @@ int cull_stage_out(sb_context* c, const sb_cull_params* p, sb_cull_data* d, cons
     return SB_OK;
 }
 
+// The median pass as a parallel fixpoint (cull_fix_kernel).  Returns
+// SB_ERR_UNSUPPORTED, with offR/offA untouched, when it has not converged
+// after kMaxFixSteps steps (or the box is too large for the warp medians):
+// the caller then runs the wavefront kernel.
+constexpr int kMaxFixSteps = 48;
+int run_st_fixpoint(sb_context* c, const sb_cull_params* p, sb_cull_data* d, const CullDev* v, int nv, int* ctl)
+{
+    if (nv > 4) return SB_ERR_UNSUPPORTED;
+    const long long n = (long long)p->nR * p->nA;
+    cudaError_t e;
+    uint8_t* fl = (uint8_t*)sb_ctx_buf(c, "c_fix", (size_t)n * 4, &e);
+    if (!fl) return sb_ctx_fail(c, SB_ERR_NOMEM, "device allocation failed");
+    uint8_t* C[2] = {fl, fl + n};
+    uint8_t* G[2] = {fl + 2 * n, fl + 3 * n};
+    unsigned int* nChanged = (unsigned int*)(ctl + 2);
+    cudaStream_t s = c->stream;
+    CKC(cudaMemsetAsync(C[0], 0, (size_t)n, s), "memset");
+    FixArgs f;
+    f.offR = v->offR; f.offA = v->offA;
+    f.nR = p->nR; f.nA = p->nA; f.bR = p->bR; f.bA = p->bA; f.nGood = p->nGood;
+    f.maxA = p->maxA; f.maxR = p->maxR;
+    f.nChanged = nChanged;
+    const int threads = 256;
+    long long blocks = (n * 32 + threads - 1) / threads;
+    if (blocks > (long long)c->numSM * 64) blocks = (long long)c->numSM * 64;
+    int cur = 0;
+    for (int step = 0; step < kMaxFixSteps; ++step) {
+        f.cin = C[cur];
+        f.cout = C[cur ^ 1];
+        f.chgIn = step == 0 ? nullptr : G[cur];
+        f.chgOut = G[cur ^ 1];
+        CKC(cudaMemsetAsync(nChanged, 0, sizeof(unsigned int), s), "memset");
+        switch (nv) {
+        case 1: cull_fix_kernel<1><<<(int)blocks, threads, 0, s>>>(f); break;
+        case 2: cull_fix_kernel<2><<<(int)blocks, threads, 0, s>>>(f); break;
+        case 3: cull_fix_kernel<3><<<(int)blocks, threads, 0, s>>>(f); break;
+        default: cull_fix_kernel<4><<<(int)blocks, threads, 0, s>>>(f); break;
+        }
+        CKC(cudaGetLastError(), "cull_fix");
+        c->launches++;
+        unsigned int changed = 0;
+        CKC(cudaMemcpyAsync(&changed, nChanged, sizeof(changed), cudaMemcpyDeviceToHost, s), "d2h");
+        CKC(cudaStreamSynchronize(s), "cull_fix");
+        cur ^= 1;
+        if (changed == 0) {
+            unsigned long long* nCulled = (unsigned long long*)(ctl + 4);
+            long long ab = (n + 255) / 256;
+            if (ab > (long long)c->numSM * 16) ab = (long long)c->numSM * 16;
+            cull_apply_kernel<<<(int)ab, 256, 0, s>>>(v->offR, v->offA, C[cur], n, nCulled);
+            CKC(cudaGetLastError(), "cull_apply");
+            c->launches++;
+            unsigned long long culled = 0;
+            CKC(cudaMemcpyAsync(&culled, nCulled, sizeof(culled), cudaMemcpyDeviceToHost, s), "d2h");
+            CKC(cudaStreamSynchronize(s), "cull_apply");
+            d->nCulled = (int64_t)culled;
+            return SB_OK;
+        }
+    }
+    return SB_ERR_UNSUPPORTED;
+}
+
 int run_st_data(sb_context* c, const sb_cull_params* p, sb_cull_data* d, const CullDev* v)
 {
     const int n = p->nR * p->nA;
@@ -629,9 +802,14 @@ int run_st_data(sb_context* c, const sb_cull_params* p, sb_cull_data* d, const C
     cull_prepass_kernel<<<(n + 255) / 256, 256, 0, s>>>(a);
     CKC(cudaGetLastError(), "cull_prepass");
     c->launches++;
-    // one warp per row in flight; enough warps for the wavefront depth
     const int box = (p->bR / 2 * 2 + 1) * (p->bA / 2 * 2 + 1);
     const int nv = (box + 31) / 32;
+    // parallel fixpoint first (exact when it converges), the wavefront if not
+    {
+        int rc = run_st_fixpoint(c, p, d, v, nv, ctl);
+        if (rc != SB_ERR_UNSUPPORTED) return rc;
+    }
+    // one warp per row in flight; enough warps for the wavefront depth
     int warps = c->numSM * 32;
     if (warps > p->nA) warps = p->nA;
     const int threads = 128, blocks = (warps * 32 + threads - 1) / threads;

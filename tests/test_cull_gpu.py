@@ -45,6 +45,7 @@ def _check(g, o, keys_exact=("offR", "offA", "type")):
     dict(),                                                          # cullst defaults
     dict(bR=5, bA=5, nGood=12, sR=3, sA=3, islandThresh=10),          # 5x5 median, 3x3 smoothing, islands
     dict(bR=7, bA=3, nGood=5, maxA=0.5, maxR=0.5, sR=4, sA=1, corrThresh=0.2, islandThresh=4, connectivity=4),
+    dict(bR=13, bA=13, nGood=40, islandThresh=6),  # box above 128 values: the row-wavefront median kernel
 ])
 def test_cull_pipeline_matches_oracle(ctx, kw):
     nA, nR = 150, 230
