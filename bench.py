@@ -511,6 +511,78 @@ def run_serving(args):
             "peak_admitted_gb": peak / 1e9, "clocks": clk}
 
 
+def run_dftgemm(args):
+    """Comparator for the split-BF16 DFT-GEMM form of the complex stage's
+    transforms: the 2-D forward DFTs of both 64 x 64 windows and the 128 x 128
+    zero-padded inverse as real GEMMs on the tensor cores (cuBLAS through
+    torch.matmul), each complex product in the real block form
+    [[Re, -Im], [Im, Re]] and each GEMM as three bf16 products (hi*hi, hi*lo,
+    lo*hi) accumulated in fp32.  Timed on a batch of patches with the data in
+    HBM between the row and column GEMMs (a library GEMM cannot keep it on
+    chip), extrapolated to the default workload's 1,955,217 patches, and set
+    beside the FP32 complex stage, which does all of that plus the loads,
+    Doppler, peak search and oversampling."""
+    import torch
+    W = 64
+    B = args.batch
+
+    def dft(n_out, n_in, sign, pad_to=None):
+        k = torch.arange(n_out, dtype=torch.float64)[:, None]
+        t = torch.arange(n_in, dtype=torch.float64)[None, :]
+        if pad_to:  # zero-padded inverse: input bins at their padded positions
+            t = torch.where(t < n_in // 2, t, t + (pad_to - n_in))
+            n = pad_to
+        else:
+            n = n_in
+        ang = sign * 2 * np.pi * k * t / n
+        re, im = torch.cos(ang), torch.sin(ang)
+        return torch.cat([torch.cat([re, -im], 1), torch.cat([im, re], 1)], 0).float().cuda()
+
+    def split(m):
+        hi = m.to(torch.bfloat16)
+        lo = (m - hi.float()).to(torch.bfloat16)
+        return hi, lo
+
+    def gemm3(a, b):  # a: (M, K) fp32 matrix, b: (K, N) fp32
+        ah, al = split(a)
+        bh, bl = split(b)
+        c = torch.matmul(ah, bh).float()
+        c += torch.matmul(ah, bl).float()
+        c += torch.matmul(al, bh).float()
+        return c
+
+    Fw = dft(W, W, -1.0)                 # (128, 128) forward 64-point DFT, real block form
+    Iw = dft(2 * W, W, 1.0, pad_to=2 * W)  # (256, 128) zero-padded inverse 64 -> 128
+    x = torch.randn(2 * W, W * 2 * B, device="cuda")  # both windows of B patches: [Re; Im] x (W columns)
+    s = torch.randn(2 * W, W * B, device="cuda")
+    torch.cuda.synchronize()
+
+    def step():
+        y = gemm3(Fw, x)                                   # forward along one axis
+        y = y.reshape(2 * W, 2 * B, W).transpose(0, 2).reshape(2 * W, -1).contiguous()
+        y = gemm3(Fw, y)                                   # forward along the other axis
+        z = gemm3(Iw, s)                                   # padded inverse rows (64 -> 128)
+        z = z.reshape(4 * W, B, W).permute(2, 1, 0).reshape(2 * W, -1).contiguous()
+        z = gemm3(Iw, z)                                   # padded inverse columns
+        return y, z
+
+    for _ in range(2):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    full = N_A * N_R
+    return {"workload": f"split-BF16 DFT-GEMM comparator: 64x64 forward x2 + 128x128 padded inverse per patch, "
+                        f"batch {B} patches, cuBLAS bf16 (3 products, fp32 accumulate)",
+            "ms_per_batch": ms, "ms_extrapolated_1955217_patches": ms * full / B,
+            "transforms_only": True, "unit": "ms"}
+
+
 def run_other(args):
     import torch
     from specklesource_b200 import abi, runtime, synth
@@ -572,6 +644,8 @@ def run_other(args):
                       "cpu_baseline": {"value": cpu, "unit": "patches/s", "cores": cores, "kind": "port",
                                        "sample": f"{cores} x 12 points spread over the grid, f32 CPU restatement"},
                       "clocks": clk})
+    elif args.workload == "dftgemm":
+        lines.append(run_dftgemm(args))
     elif args.workload in ("cfg4", "cfg5"):
         lines.append(run_batched(args) if args.workload == "cfg4" else run_serving(args))
     elif args.workload == "cull":
@@ -615,14 +689,15 @@ def main():
     ap.add_argument("--no-accuracy", action="store_true", help="skip the FP64-oracle check of a row sample")
     ap.add_argument("--slots", type=int, default=4, help="job-server slots for --workload cfg4/cfg5")
     ap.add_argument("--jobs", type=int, default=200, help="jobs offered in --workload cfg5")
-    ap.add_argument("--workload", default="large", choices=["large", "small", "cfg1", "cfg3", "cfg3small", "cfg4", "cfg5", "cull"],
+    ap.add_argument("--batch", type=int, default=32768, help="patches per batch in --workload dftgemm")
+    ap.add_argument("--workload", default="large", choices=["large", "small", "cfg1", "cfg3", "cfg3small", "cfg4", "cfg5", "cull", "dftgemm"],
                     help="small: 2400x4800 profiling case of the same generator; cfg1 / cfg3 / cull: the "
                          "other configurations (one JSON line each, not the bench line); cfg3small: the cfg3 "
                          "geometry on a 2000x4000 pair (profiling case)")
     args = ap.parse_args()
     if args.workload == "small":
         use_small_workload()
-    if args.workload in ("cfg1", "cfg3", "cfg3small", "cfg4", "cfg5", "cull"):
+    if args.workload in ("cfg1", "cfg3", "cfg3small", "cfg4", "cfg5", "cull", "dftgemm"):
         return run_other(args)
     if args.impl == "reference":
         return run_reference(args)

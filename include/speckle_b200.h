@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define SB_ABI_VERSION 1
+#define SB_ABI_VERSION 2
 
 /* Status codes. */
 #define SB_OK 0
@@ -139,6 +139,20 @@ typedef struct {
     const double *overRange;
 } sb_baseline;
 
+/* Multi-looked interferogram used to flatten the fringe phase of patch 1
+ * before complex matching (the intfile / intgeodat inputs; read by getInt,
+ * Strack/getInt.c:11-77, applied by phaseCorrectInt,
+ * Strack/speckleTrack.c:909-1000).  Samples are complex int16 (re, im pairs),
+ * na x nr, each covering nrl x nal SLC pixels.  Lines the reference finds
+ * missing from a short file hold (1, 1); pass them that way. */
+typedef struct {
+    const void *data;  /* na * nr (re, im) int16 pairs */
+    int32_t nr, na;    /* size (the geodat's rangeSize / azimuthSize) */
+    int32_t nrl, nal;  /* range / azimuth looks */
+    int32_t byteOrder; /* SB_MSB as in the file (freadBS), or SB_LSB */
+    int32_t onDevice;  /* data is a device pointer */
+} sb_interferogram;
+
 /* Parameters shared by strack and strackw (TrackParams, Strack/strack.h:56-165). */
 typedef struct {
     int32_t rStart, aStart; /* first estimate (already divided by scaleFactor) */
@@ -164,6 +178,7 @@ typedef struct {
     const sb_offset_grid *initOffsets; /* required when polyShift == 0 */
     const sb_mask *mask;               /* NULL: every point is tried */
     const sb_baseline *baseline;       /* NULL: zero baseline */
+    const sb_interferogram *intf;      /* NULL: no interferogram (strack complex stage only) */
 } sb_track_params;
 
 /* ------------------------------------------------------------------------ */

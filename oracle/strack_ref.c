@@ -101,6 +101,10 @@ typedef struct {
     offt2d *cForwardIn, *cReverseNoPad, *cForwardFast, *cReverseFast;
     ocplx *cFast, *psFast, *psFastOver, *cFastOver;
     AmpBufs amp[2];
+    /* interferogram phase correction (initPhaseCorrect, speckleTrack.c:1576-1601) */
+    int intPs, intPSA, intPSR;
+    ocplx *intPatch, *fftIntPatch, *fftIntPatchOver, *intPatchOver;
+    offt2d *intForward, *intBackward;
     float *aZDefocus; /* output grid */
     int64_t nComplex, nAmp, nAmpL, nFail;
 } StCtx;
@@ -610,6 +614,75 @@ static void phaseCorrectBaseline(StCtx *c, int r1, int a1)
     }
 }
 
+/* Interferogram sample (getInt, Strack/getInt.c:66-73: int16 pairs read with
+ * byte swapping when the file is big-endian, converted to float). */
+static void int_sample(const sb_interferogram *f, int row, int col, REAL *re, REAL *im)
+{
+    const unsigned char *b = (const unsigned char *)f->data + ((size_t)row * f->nr + col) * 4;
+    int16_t r, i;
+    if (f->byteOrder == SB_MSB) {
+        r = (int16_t)((b[0] << 8) | b[1]);
+        i = (int16_t)((b[2] << 8) | b[3]);
+    } else {
+        r = (int16_t)((b[1] << 8) | b[0]);
+        i = (int16_t)((b[3] << 8) | b[2]);
+    }
+    *re = (REAL)(float)r;
+    *im = (REAL)(float)i;
+}
+
+static void phaseCorrectInt(StCtx *c, int r1, int a1)
+{
+    /* speckleTrack.c:909-1000, osF = 1 */
+    const sb_interferogram *f = c->p->intf;
+    if (f == NULL || c->intPs == 0) return;
+    const int ps = c->intPs, pSA = c->intPSA, pSR = c->intPSR;
+    const int ia1 = (a1 + c->wA / 2) / f->nal - ps / 2;
+    const int ir1 = (r1 + c->wR / 2) / f->nrl - ps / 2;
+    if (!inBounds(ir1, ia1, ps, ps, f->nr, f->na)) return;
+    for (int i = 0; i < ps; i++)
+        for (int j = 0; j < ps; j++)
+            int_sample(f, ia1 + i, ir1 + j, &c->intPatch[i * ps + j].re, &c->intPatch[i * ps + j].im);
+    offt2d_exec(c->intForward, c->intPatch, c->fftIntPatch);
+    double maxf = 0.;
+    for (int k = 0; k < ps * ps; k++) {
+        const double p = (double)c->fftIntPatch[k].re * c->fftIntPatch[k].re +
+                         (double)c->fftIntPatch[k].im * c->fftIntPatch[k].im;
+        maxf = maxf > p ? maxf : p;
+    }
+    /* The reference's loop body has no braces: the real part is cleared
+       below 0.99 of the peak power, the imaginary part of every bin is cleared. */
+    for (int k = 0; k < ps * ps; k++) {
+        const double p = (double)c->fftIntPatch[k].re * c->fftIntPatch[k].re +
+                         (double)c->fftIntPatch[k].im * c->fftIntPatch[k].im;
+        if (p < 0.99 * maxf) c->fftIntPatch[k].re = 0.0;
+        c->fftIntPatch[k].im = 0.0;
+    }
+    zeroPadFFT(c->fftIntPatchOver, pSA, pSR, c->fftIntPatch, ps, ps, 0, 0);
+    offt2d_exec(c->intBackward, c->fftIntPatchOver, c->intPatchOver);
+    int i1 = pSA / 2 - c->wA / 2;
+    for (int i = 0; i < c->wA; i++) {
+        int j1 = pSR / 2 - c->wR / 2;
+        for (int j = 0; j < c->wR; j++) {
+            double pr = c->intPatchOver[(size_t)i1 * pSR + j1].re;
+            double pi = -c->intPatchOver[(size_t)i1 * pSR + j1].im;
+            double scale;
+            if (fabs(pr) < 1.0e-6 && fabs(pi) < 1.0e-6) {
+                pr = 1.0;
+                pi = 0.0;
+                scale = 1.0;
+            } else
+                scale = 1.0 / sqrt(pr * pr + pi * pi);
+            ocplx *q = &c->patch1[i * c->wR + j];
+            const double cr = q->re, ci = q->im;
+            q->re = (REAL)((cr * pr - ci * pi) * scale);
+            q->im = (REAL)((cr * pi + ci * pr) * scale);
+            j1++;
+        }
+        i1++;
+    }
+}
+
 static void cmpPSWithPad(StCtx *c)
 {
     /* speckleTrack.c:604-643 */
@@ -687,6 +760,7 @@ static int complexMatch(StCtx *c, int r1, int a1, int *iMax, int *jMax, double *
     double wRover2exp = c->wR / 2. * NOVER * OSA;
     double wAover2exp = c->wA / 2. * NOVER * OSA;
     phaseCorrectBaseline(c, r1, a1);
+    phaseCorrectInt(c, r1, a1);
     cmpPSWithPad(c);
     cmpTrackFast(c, iMax, jMax, cMax);
     good = FALSE;
@@ -836,6 +910,9 @@ int oracle_strack(const sb_track_params *p, const sb_image *img1, const sb_image
     if (p->gaussFlag) return SB_ERR_UNSUPPORTED;
     if (p->hanningFlag && p->wR != p->wA) return SB_ERR_UNSUPPORTED;
     if (p->polyShift == 0 && p->initOffsets == NULL) return SB_ERR_ARG;
+    if (p->intf && (p->intf->nal <= 0 || p->intf->nrl <= 0 || p->intf->nr <= 0 || p->intf->na <= 0 ||
+                    !p->intf->data || p->intf->onDevice))
+        return SB_ERR_ARG;
     StCtx C, *c = &C;
     memset(c, 0, sizeof(C));
     c->p = p;
@@ -858,6 +935,26 @@ int oracle_strack(const sb_track_params *p, const sb_image *img1, const sb_image
     ampAlloc(&c->amp[0], p->wRa, p->wAa);
     ampAlloc(&c->amp[1], p->wRa * LA, p->wAa * LA);
     if (p->hanningFlag == TRUE && p->noComplex == FALSE) computeHanning(c);
+    if (p->intf != NULL && p->noComplex == FALSE) {
+        /* initPhaseCorrect: patch of max(wA/nal, wR/nrl, INTPATCHSIZE = 8) samples */
+        const sb_interferogram *f = p->intf;
+        int ps = wA / f->nal > wR / f->nrl ? wA / f->nal : wR / f->nrl;
+        ps = ps > 8 ? ps : 8;
+        /* a padded patch smaller than the window makes the reference read
+           outside it (speckleTrack.c:978-983): refused */
+        if (ps * f->nal < wA || ps * f->nrl < wR) {
+            free(c->hanning); /* the rest is released by the process; test infrastructure */
+            return SB_ERR_UNSUPPORTED;
+        }
+        c->intPs = ps;
+        c->intPSA = ps * f->nal;
+        c->intPSR = ps * f->nrl;
+        c->intPatch = cbuf((size_t)ps * ps); c->fftIntPatch = cbuf((size_t)ps * ps);
+        c->fftIntPatchOver = cbuf((size_t)c->intPSA * c->intPSR);
+        c->intPatchOver = cbuf((size_t)c->intPSA * c->intPSR);
+        c->intForward = offt2d_plan(ps, ps, OFFT_FORWARD);
+        c->intBackward = offt2d_plan(c->intPSA, c->intPSR, OFFT_BACKWARD);
+    }
 
     const int nR = p->nR, nA = p->nA;
     if (row1 <= 0 || row1 > nA) row1 = nA;
@@ -970,6 +1067,10 @@ int oracle_strack(const sb_track_params *p, const sb_image *img1, const sb_image
     free(c->cFast); free(c->psFast); free(c->psFastOver); free(c->cFastOver);
     ampFree(&c->amp[0]);
     ampFree(&c->amp[1]);
+    if (c->intPs) {
+        free(c->intPatch); free(c->fftIntPatch); free(c->fftIntPatchOver); free(c->intPatchOver);
+        offt2d_destroy(c->intForward); offt2d_destroy(c->intBackward);
+    }
     return SB_OK;
 }
 

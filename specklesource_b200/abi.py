@@ -71,6 +71,16 @@ class SbBaseline(C.Structure):
     ]
 
 
+class SbInterferogram(C.Structure):
+    _fields_ = [
+        ("data", C.c_void_p),
+        ("nr", _i32), ("na", _i32),
+        ("nrl", _i32), ("nal", _i32),
+        ("byteOrder", _i32),
+        ("onDevice", _i32),
+    ]
+
+
 class SbTrackParams(C.Structure):
     _fields_ = [
         ("rStart", _i32), ("aStart", _i32),
@@ -93,6 +103,7 @@ class SbTrackParams(C.Structure):
         ("initOffsets", C.POINTER(SbOffsetGrid)),
         ("mask", C.POINTER(SbMask)),
         ("baseline", C.POINTER(SbBaseline)),
+        ("intf", C.POINTER(SbInterferogram)),
     ]
 
 
@@ -191,6 +202,7 @@ class TrackParams:
         self.aShiftPoly = (0.0, 0.0, 0.0)
         self.initOffsets = None  # dict(nr, na, r0, a0, deltaR, deltaA, dr, da)
         self.mask = None  # dict(r0, a0, nr, na, nrl, nal, mask)
+        self.intf = None  # dict(data=int16 (na, nr, 2) array, nrl, nal[, byteOrder])
         for k, v in kw.items():
             if not hasattr(self, k):
                 raise TypeError(f"unknown track parameter {k!r}")
@@ -201,7 +213,7 @@ class TrackParams:
         p = SbTrackParams()
         keep = []
         for name, _ in SbTrackParams._fields_:
-            if name in ("rShiftPoly", "aShiftPoly", "initOffsets", "mask", "baseline"):
+            if name in ("rShiftPoly", "aShiftPoly", "initOffsets", "mask", "baseline", "intf"):
                 continue
             setattr(p, name, getattr(self, name))
         for i in range(3):
@@ -222,6 +234,20 @@ class TrackParams:
                         int(m["nal"]), ptr(mk))
             keep += [mk, sm]
             p.mask = C.pointer(sm)
+        if self.intf is not None:
+            f = self.intf
+            d = f["data"]
+            if isinstance(d, np.ndarray):
+                d = np.ascontiguousarray(d)
+                order = SB_MSB if d.dtype.byteorder == ">" else SB_LSB
+                na, nr = d.shape[:2]
+                g = SbInterferogram(ptr(d), nr, na, int(f["nrl"]), int(f["nal"]), f.get("byteOrder", order), 0)
+            else:  # torch CUDA int16 tensor (na, nr, 2), native order
+                na, nr = d.shape[:2]
+                g = SbInterferogram(d.data_ptr(), nr, na, int(f["nrl"]), int(f["nal"]), f.get("byteOrder", SB_LSB),
+                                    1)
+            keep += [d, g]
+            p.intf = C.pointer(g)
         return p, keep
 
 

@@ -508,6 +508,22 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
         if (p->maxTries > 1 && !amp_supported(WA * LA))
             return sb_ctx_fail(c, SB_ERR_UNSUPPORTED, "large amplitude window %d not supported", WA * LA);
     }
+    // interferogram (initPhaseCorrect, speckleTrack.c:1576-1601): patch of
+    // max(wA/nal, wR/nrl, 8) samples, padded to (ps nal) x (ps nrl)
+    int intPs = 0;
+    if (p->intf && p->noComplex == 0) {
+        const sb_interferogram* fi = p->intf;
+        if (!fi->data || fi->nr <= 0 || fi->na <= 0 || fi->nrl <= 0 || fi->nal <= 0)
+            return sb_ctx_fail(c, SB_ERR_ARG, "invalid interferogram");
+        intPs = p->wA / fi->nal > p->wR / fi->nrl ? p->wA / fi->nal : p->wR / fi->nrl;
+        intPs = intPs > 8 ? intPs : 8;
+        if (intPs * fi->nal < p->wA || intPs * fi->nrl < p->wR)
+            return sb_ctx_fail(c, SB_ERR_UNSUPPORTED,
+                               "interferogram looks (%d, %d) give a padded patch smaller than the window (the "
+                               "reference reads outside it)", fi->nrl, fi->nal);
+        if (2 * intPs * intPs > W * (W + 1) || intPs * fi->nal >= 32768 || intPs * fi->nrl >= 32768)
+            return sb_ctx_fail(c, SB_ERR_UNSUPPORTED, "interferogram patch %d too large for window %d", intPs, W);
+    }
     const sb_baseline* bl = p->baseline;
     const int baseOn =
         bl && (bl->Bn != 0 || bl->Bp != 0 || bl->dBn != 0 || bl->dBp != 0 || bl->dBnQ != 0 || bl->dBpQ != 0);
@@ -631,6 +647,26 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
         }
         a.rec = drec;
         a.fit = dfit;
+        if (p->intf) {
+            // phaseCorrectInt: the interferogram on the device, patch geometry
+            const sb_interferogram* fi = p->intf;
+            const size_t ib = (size_t)fi->nr * fi->na * 4;
+            const uint32_t* di = (const uint32_t*)fi->data;
+            if (!fi->onDevice) {
+                uint32_t* buf = (uint32_t*)sb_ctx_buf(c, "intf", ib, &e);
+                if (!buf) return sb_ctx_fail(c, SB_ERR_NOMEM, "device allocation failed");
+                CK(cudaMemcpyAsync(buf, fi->data, ib, cudaMemcpyHostToDevice, c->stream), "interferogram");
+                di = buf;
+            }
+            a.intf = di;
+            a.intNr = fi->nr; a.intNa = fi->na; a.intNrl = fi->nrl; a.intNal = fi->nal;
+            a.intMSB = fi->byteOrder == SB_MSB;
+            a.intPs = intPs;
+            a.intPSA = intPs * fi->nal;
+            a.intPSR = intPs * fi->nrl;
+            a.twP = tw_table(c, intPs);
+            if (!a.twP) return sb_ctx_fail(c, SB_ERR_NOMEM, "table allocation failed");
+        }
         if (!a.twW || !a.tau || !a.osA || !a.osD || (p->hanningFlag && !a.hanning))
             return sb_ctx_fail(c, SB_ERR_NOMEM, "table allocation failed");
         int bpsm = cmplx_blocks_per_sm(W);

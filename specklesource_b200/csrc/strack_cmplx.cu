@@ -145,6 +145,142 @@ __device__ __forceinline__ void cpeak_from_planes(const float* smf, float pmax, 
     jMax = ij % W + ((q == 1 || q == 3) ? W : 0);
 }
 
+// phaseCorrectInt (Strack/speckleTrack.c:909-1000) on patch 1 (X, row
+// stride RS): the ps x ps interferogram patch centred on the window is
+// transformed, every bin below 0.99 of the peak power loses its real part and
+// every bin its imaginary part (the reference's loop has no braces), the
+// remaining bins are placed as zeroPadFFT places them in a (ps nal) x (ps nrl)
+// array (for odd ps the last row and column are not copied) and the inverse
+// transform is evaluated directly at the window's pixels; patch 1 is
+// multiplied by conj(P) / |P| (or left alone where |P| < 1e-6).  The small
+// forward DFT and the peak list use `work` (2 ps^2 float2, the free Y buffer).
+template <int W, int RS, int NT>
+__device__ __forceinline__ void phase_correct_int(const CmplxArgs& a, const PointPlan& pl, float2* X, float2* work,
+                                                  double* red)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int ps = a.intPs;
+    const int ia1 = (pl.a1 + W / 2) / a.intNal - ps / 2;
+    const int ir1 = (pl.r1 + W / 2) / a.intNrl - ps / 2;
+    if (!(ir1 > 0 && ir1 + ps < a.intNr && ia1 > 0 && ia1 + ps < a.intNa)) return;  // inBounds, uniform
+    const int n2 = ps * ps;
+    float2* G = work;       // interferogram patch, then its spectrum
+    float2* H = work + n2;  // row transform; then the peak list
+    for (int e = tid; e < n2; e += NT) {
+        uint32_t w = __ldg(a.intf + (size_t)(ia1 + e / ps) * a.intNr + ir1 + e % ps);
+        if (a.intMSB) w = bswap16x2(w);
+        G[e] = make_float2((float)(int16_t)(w & 0xffffu), (float)(int16_t)(w >> 16));
+    }
+    __syncthreads();
+    for (int e = tid; e < n2; e += NT) {  // rows: H[i][k] = sum_j G[i][j] W^{jk}
+        const int i = e / ps, k = e % ps;
+        float2 acc = make_float2(0.f, 0.f);
+        int t = 0;
+        for (int j = 0; j < ps; ++j) {
+            const float2 g = G[i * ps + j], w = a.twP[t];
+            acc.x = fmaf(g.x, w.x, fmaf(-g.y, w.y, acc.x));
+            acc.y = fmaf(g.x, w.y, fmaf(g.y, w.x, acc.y));
+            t += k;
+            t = t >= ps ? t - ps : t;
+        }
+        H[e] = acc;
+    }
+    __syncthreads();
+    double pmax = 0.0;
+    for (int e = tid; e < n2; e += NT) {  // columns: F[k1][k2] = sum_i H[i][k2] W^{i k1}
+        const int k1 = e / ps, k2 = e % ps;
+        float2 acc = make_float2(0.f, 0.f);
+        int t = 0;
+        for (int i = 0; i < ps; ++i) {
+            const float2 h = H[i * ps + k2], w = a.twP[t];
+            acc.x = fmaf(h.x, w.x, fmaf(-h.y, w.y, acc.x));
+            acc.y = fmaf(h.x, w.y, fmaf(h.y, w.x, acc.y));
+            t += k1;
+            t = t >= ps ? t - ps : t;
+        }
+        G[e] = acc;
+        pmax = fmax(pmax, (double)acc.x * acc.x + (double)acc.y * acc.y);
+    }
+    // block maximum of the bin power (double, non-negative: bits order as values)
+    {
+        unsigned long long u = (unsigned long long)__double_as_longlong(pmax);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long v = __shfl_xor_sync(0xffffffffu, u, o);
+            u = v > u ? v : u;
+        }
+        unsigned long long* sc = reinterpret_cast<unsigned long long*>(red);
+        if (lane == 0) sc[warp] = u;
+        __syncthreads();
+        u = sc[0];
+#pragma unroll
+        for (int w = 1; w < NT / 32; ++w) u = sc[w] > u ? sc[w] : u;
+        __syncthreads();
+        pmax = __longlong_as_double((long long)u);
+    }
+    // the surviving bins (real parts), in bin order, as (value, padded K1, K2)
+    float* lv = reinterpret_cast<float*>(H);
+    int* lk = reinterpret_cast<int*>(H) + n2;
+    int* cntp = reinterpret_cast<int*>(red);
+    const int h = ps / 2;
+    if (warp == 0) {
+        int cnt = 0;
+        for (int e0 = 0; e0 < n2; e0 += 32) {
+            const int e = e0 + lane;
+            bool keep = false;
+            float v = 0.f;
+            int K = 0;
+            if (e < n2) {
+                const float2 f = G[e];
+                const double p = (double)f.x * f.x + (double)f.y * f.y;
+                const int k1 = e / ps, k2 = e % ps;
+                v = p < 0.99 * pmax ? 0.f : f.x;
+                const bool in1 = k1 < 2 * h, in2 = k2 < 2 * h;  // zeroPadFFT copies 2 (ps/2) rows and columns
+                const int K1 = k1 < h ? k1 : a.intPSA - 2 * h + k1;
+                const int K2 = k2 < h ? k2 : a.intPSR - 2 * h + k2;
+                keep = v != 0.f && in1 && in2;
+                K = (K1 << 16) | K2;
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, keep);
+            if (keep) {
+                const int pos = cnt + __popc(m & ((1u << lane) - 1u));
+                lv[pos] = v;
+                lk[pos] = K;
+            }
+            cnt += __popc(m);
+        }
+        if (lane == 0) *cntp = cnt;
+    }
+    __syncthreads();
+    const int nPeak = *cntp;
+    const int i1 = a.intPSA / 2 - W / 2, j1 = a.intPSR / 2 - W / 2;
+    for (int e = tid; e < W * W; e += NT) {
+        const int i = e / W, j = e % W;
+        float pr = 0.f, pim = 0.f;
+        for (int q = 0; q < nPeak; ++q) {
+            const int K1 = lk[q] >> 16, K2 = lk[q] & 0xffff;
+            const int m1 = (int)(((long long)K1 * (i1 + i)) % a.intPSA);
+            const int m2 = (int)(((long long)K2 * (j1 + j)) % a.intPSR);
+            const float frac = (float)m1 / (float)a.intPSA + (float)m2 / (float)a.intPSR;
+            float sn, cs;
+            sincospif(2.0f * frac, &sn, &cs);
+            pr = fmaf(lv[q], cs, pr);
+            pim = fmaf(lv[q], sn, pim);
+        }
+        float cr = pr, ci = -pim, sc;
+        if (fabsf(cr) < 1.0e-6f && fabsf(ci) < 1.0e-6f) {
+            cr = 1.f;
+            ci = 0.f;
+            sc = 1.f;
+        } else {
+            sc = 1.0f / sqrtf(cr * cr + ci * ci);
+        }
+        const float2 z = X[i * RS + j];
+        X[i * RS + j] = make_float2((z.x * cr - z.y * ci) * sc, (z.x * ci + z.y * cr) * sc);
+    }
+    __syncthreads();
+}
+
 template <int W, int NT, bool F32>
 __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(CmplxArgs a)
 {
@@ -272,6 +408,7 @@ __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(Cmp
             }
             __syncthreads();
         }
+        if (a.intf) phase_correct_int<W, RS, NT>(a, pl, X, Y, red);
         // ---------------------------------------------------- spectra of both patches (X and Z)
         sbfft::fft2d_smem<W, -1, 2, NT, RS, 2 * IMG>(X, twW);
         // ---------------------------------------------------- padded inverse

@@ -32,6 +32,11 @@ struct CmplxArgs {
     const double* overRange;
     PointRec* rec;
     FitJob* fit;  // one entry per list position
+    // interferogram phase correction (phaseCorrectInt); intf null: none
+    const uint32_t* intf;  // na x nr (re, im) int16 pairs, one word each
+    int intNr, intNa, intNrl, intNal, intMSB;
+    int intPs, intPSA, intPSR;  // patch, padded sizes (ps * nal, ps * nrl)
+    const float2* twP;          // exp(-2 pi i e / ps), e < ps
 };
 
 // Arguments of an amplitude try (small: s = 1, large: s = LA = 2).

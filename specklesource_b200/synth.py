@@ -177,3 +177,19 @@ def offsets_field(nA, nR, seed, outliers=0.08, holes=0.02):
     mt = rng.integers(1, 4, (nA, nR)).astype(np.uint8)
     mt[f] = 0
     return offR.astype(np.float32), offA.astype(np.float32), corr, mt
+
+
+def fringe_interferogram(na, nr, nrl, nal, ramp_r, ramp_a=0.0, amp=1000.0, byte_order=">"):
+    """Multi-looked interferogram of a linear fringe, as getInt reads it:
+    complex int16 (re, im) samples, (na // nal) x (nr // nrl), sample (i, k)
+    covering SLC rows i*nal.. and columns k*nrl..; phase -(ramp_r x + ramp_a y)
+    at its first pixel, the phase of s1 conj(s2) for a pair whose secondary
+    image carries exp(+i (ramp_r x + ramp_a y)).  The fringe must stay below
+    pi per look (|ramp_r| nrl, |ramp_a| nal < pi) to be representable."""
+    ia = np.arange(na // nal)[:, None] * nal
+    ir = np.arange(nr // nrl)[None, :] * nrl
+    ph = -(ramp_r * ir + ramp_a * ia)
+    out = np.empty((na // nal, nr // nrl, 2), np.float64)
+    out[..., 0] = amp * np.cos(ph)
+    out[..., 1] = amp * np.sin(ph)
+    return np.round(out).astype(byte_order + "i2")

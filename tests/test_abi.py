@@ -41,7 +41,7 @@ def test_every_declared_symbol_is_exported(lib):
 
 
 def test_abi_version(lib):
-    assert lib.sb_abi_version() == 1
+    assert lib.sb_abi_version() == 2
 
 
 def test_context_without_device_reports_error(lib):
@@ -58,6 +58,7 @@ _STRUCTS = {
     "sb_offset_grid": abi.SbOffsetGrid,
     "sb_mask": abi.SbMask,
     "sb_baseline": abi.SbBaseline,
+    "sb_interferogram": abi.SbInterferogram,
     "sb_track_params": abi.SbTrackParams,
     "sb_track_result": abi.SbTrackResult,
     "sb_cull_params": abi.SbCullParams,

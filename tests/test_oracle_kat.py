@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle
-from specklesource_b200 import abi
+from specklesource_b200 import abi, synth
 
 LARGE = float(abi.SB_LARGEINT)
 
@@ -231,3 +231,26 @@ def test_cull_islands_by_extent_and_last_label():
     assert (out[27:29, 27:29] == 1.0).all()
     assert cd.nIslands == 1
     del d, r
+
+
+def test_interferogram_flattening_restores_matches():
+    """phaseCorrectInt: a 0.6 rad/px range fringe between the images shifts
+    their spectra apart and destroys the complex correlation; with the
+    interferogram describing it, every point matches at the true offsets."""
+    s1, s2 = synth.make_pair(256, 512, 11, dr=lambda y, x: 1.3 + 0 * x, da=lambda y, x: 0.4 + 0 * x,
+                             coherence=0.8, ramp=0.6)
+    a, b = synth.to_numpy(s1), synth.to_numpy(s2)
+    intf = synth.fringe_interferogram(256, 512, 4, 2, 0.6)
+    base = dict(rStart=40, aStart=40, deltaR=16, deltaA=16, nR=27, nA=12, wR=32, wA=32, wRa=32, wAa=32, maxTries=0)
+    plain = oracle.strack(abi.TrackParams(**base), a, b)
+    flat = oracle.strack(abi.TrackParams(**base, intf=dict(data=intf, nrl=4, nal=2)), a, b)
+    assert (plain["type"] == 1).mean() < 0.1
+    m = flat["type"] == 1
+    assert m.all()
+    assert abs(np.median(flat["offR"][m]) - 1.3) < 0.05 and abs(np.median(flat["offA"][m]) - 0.4) < 0.05
+    # a little-endian copy of the same interferogram gives the same result
+    flat2 = oracle.strack(abi.TrackParams(**base, intf=dict(data=intf.astype("<i2"), nrl=4, nal=2)), a, b)
+    assert np.array_equal(flat["offR"], flat2["offR"])
+    # looks that make the padded patch smaller than the window are refused
+    with pytest.raises(RuntimeError):
+        oracle.strack(abi.TrackParams(**base, intf=dict(data=intf, nrl=3, nal=3)), a, b)

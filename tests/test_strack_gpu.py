@@ -164,3 +164,27 @@ def test_banded_upload_matches_device_inputs(ctx, grid_plan):
     for k in ("offR", "offA", "corr", "azd", "type"):
         assert np.array_equal(out[k].cpu().numpy(), g[k]), k
     assert (g["type"] > 0).mean() > 0.9
+
+
+def test_interferogram_phase_correction(ctx):
+    """phaseCorrectInt on the GPU against the oracle: a 0.6 rad/px range fringe
+    that decorrelates the pair is flattened with the interferogram (big-endian
+    host copy and little-endian device copy give the same offsets)."""
+    import torch
+    s1, s2 = synth.make_pair(512, 1024, 12, dr=lambda y, x: 1.3 + 0.3 * torch.sin(x / 150.0),
+                             da=lambda y, x: 0.4 + 0 * x, coherence=0.8, ramp=0.6)
+    a, b = synth.to_numpy(s1), synth.to_numpy(s2)
+    intf = synth.fringe_interferogram(512, 1024, 4, 2, 0.6)
+    for W, nrl, nal in ((32, 4, 2), (64, 4, 2)):
+        kw = dict(rStart=W + 8, aStart=W + 8, deltaR=W // 2, deltaA=W // 2, nR=(1024 - 2 * W - 16) // (W // 2),
+                  nA=(512 - 2 * W - 16) // (W // 2), wR=W, wA=W, wRa=W, wAa=W)
+        fi = synth.fringe_interferogram(512, 1024, nrl, nal, 0.6)
+        p = abi.TrackParams(**kw, intf=dict(data=fi, nrl=nrl, nal=nal))
+        g, o, st = _check(ctx, p, a, b)
+        assert (o["type"] == 1).mean() > 0.9 and (g["type"] == 1).mean() > 0.9
+        td = torch.from_numpy(np.ascontiguousarray(fi.astype("<i2"))).cuda()
+        g2 = ctx.strack(abi.TrackParams(**kw, intf=dict(data=td, nrl=nrl, nal=nal)), a, b)
+        assert np.array_equal(g2["offR"], g["offR"]) and np.array_equal(g2["type"], g["type"])
+    with pytest.raises(Exception, match="smaller than the window"):
+        ctx.strack(abi.TrackParams(rStart=48, aStart=48, deltaR=16, deltaA=16, nR=4, nA=4,
+                                   intf=dict(data=intf, nrl=3, nal=3)), a, b)
