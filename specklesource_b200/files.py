@@ -11,7 +11,7 @@ import os
 import numpy as np
 
 # the keys parseTrack reads, in its order
-TRACK_KEYS = ("image1", "image2", "outputfile", "initialoffsetfile", "initShift", "intgeodat", "baseparams",
+TRACK_KEYS = ("image1", "image2", "outputfile", "initialoffsetfile", "initShift", "intfile", "intgeodat", "baseparams",
               "offsetmaskfile", "offsetmaskdat", "rstart", "astart", "deltar", "deltaa", "nR", "nA", "wr", "wa",
               "wra", "waa", "edgepad", "scalefactor", "navgR", "navgA")
 
@@ -34,6 +34,26 @@ def write_slc(path, img, byte_order="MSB"):
                 f'    <SourceFilename relativeToVRT="1">{os.path.basename(path)}</SourceFilename>\n'
                 f'    <ImageOffset>0</ImageOffset>\n    <PixelOffset>{pix}</PixelOffset>\n'
                 f'    <LineOffset>{nr * pix}</LineOffset>\n    <ByteOrder>{byte_order}</ByteOrder>\n'
+                f'  </VRTRasterBand>\n</VRTDataset>\n')
+
+
+def write_interferogram(path, data, nrl, nal, lines=None):
+    """Complex int16 interferogram (na, nr, 2) as the strack tool reads it:
+    raw samples (byte order of the array) plus <path>.vrt giving the size, the
+    byte order and the looks (metadata nRangeLooks / nAzimuthLooks).  lines:
+    write only the first `lines` rows (a short file)."""
+    data = np.ascontiguousarray(data)
+    na, nr = data.shape[:2]
+    order = "MSB" if data.dtype.byteorder == ">" else "LSB"
+    (data if lines is None else data[:lines]).tofile(path)
+    with open(path + ".vrt", "w") as f:
+        f.write(f'<VRTDataset rasterXSize="{nr}" rasterYSize="{na}">\n'
+                f'  <Metadata>\n    <MDI key="nRangeLooks">{nrl}</MDI>\n'
+                f'    <MDI key="nAzimuthLooks">{nal}</MDI>\n  </Metadata>\n'
+                f'  <VRTRasterBand dataType="CInt16" band="1" subClass="VRTRawRasterBand">\n'
+                f'    <SourceFilename relativeToVRT="1">{os.path.basename(path)}</SourceFilename>\n'
+                f'    <ImageOffset>0</ImageOffset>\n    <PixelOffset>4</PixelOffset>\n'
+                f'    <LineOffset>{nr * 4}</LineOffset>\n    <ByteOrder>{order}</ByteOrder>\n'
                 f'  </VRTRasterBand>\n</VRTDataset>\n')
 
 

@@ -10,8 +10,9 @@
  *
  * Images are raw SLC files described by a GDAL VRT sidecar (<image>.vrt).
  * GrIMP .par/geodat readers (readOldPar, parseInputFile) are not part of the
- * reference tree, so `image1par` files, geodat masks, interferograms and a
- * non-zero baseline are refused with a message.
+ * reference tree, so `image1par` files, geodat masks and a non-zero baseline
+ * are refused with a message, and an interferogram (intfile, strack only)
+ * takes its size and looks from <intfile>.vrt.
  */
 #define _GNU_SOURCE
 #include <libgen.h>
@@ -106,6 +107,52 @@ static char *suffixed(const char *base, const char *suf)
 }
 
 /* An SLC image through its VRT sidecar (checkForVrt + parseSLCVrtNew). */
+/* The interferogram for getInt (Strack/getInt.c:11-77): complex int16 samples,
+ * big-endian unless its VRT says LSB, with the size and looks that the
+ * reference takes from the intgeodat file.  GrIMP's geodat reader
+ * (parseInputFile) is not part of the reference tree, so the same facts come
+ * from <intfile>.vrt: rasterXSize/rasterYSize, dataType CInt16, ByteOrder and
+ * the metadata keys nRangeLooks / nAzimuthLooks.  As in getInt, a file with
+ * fewer lines than the raster is read as far as it goes and the missing lines
+ * hold (1, 1). */
+static void load_interferogram(const char *intFile, sb_interferogram *f)
+{
+    char vrt[4200];
+    snprintf(vrt, sizeof vrt, "%s.vrt", intFile);
+    sbio_vrt v;
+    if (!sbio_exists(vrt) || !sbio_vrt_read(vrt, &v))
+        sbio_die("getInt: %s needs a VRT sidecar %s (size, CInt16, ByteOrder, nRangeLooks, nAzimuthLooks): "
+                 "GrIMP's geodat reader is not part of the reference tree", intFile, vrt);
+    if (v.sampleType != SB_CINT16) sbio_die("getInt: %s must describe CInt16 samples", vrt);
+    const char *nrl = sbio_vrt_meta(&v, "nRangeLooks"), *nal = sbio_vrt_meta(&v, "nAzimuthLooks");
+    if (!nrl || !nal) sbio_die("getInt: %s lacks nRangeLooks / nAzimuthLooks", vrt);
+    f->nr = v.nr;
+    f->na = v.na;
+    f->nrl = atoi(nrl);
+    f->nal = atoi(nal);
+    if (f->nr <= 0 || f->na <= 0 || f->nrl <= 0 || f->nal <= 0) sbio_die("getInt: invalid size or looks in %s", vrt);
+    f->byteOrder = v.byteOrder == SB_LSB ? SB_LSB : SB_MSB;
+    f->onDevice = 0;
+    const size_t row = (size_t)f->nr * 4;
+    unsigned char *buf = malloc(row * f->na);
+    if (!buf) sbio_die("getInt: cannot allocate the interferogram buffer");
+    /* fill value (1, 1) in the file's byte order */
+    const unsigned char one[4] = {f->byteOrder == SB_MSB ? 0 : 1, f->byteOrder == SB_MSB ? 1 : 0,
+                                  f->byteOrder == SB_MSB ? 0 : 1, f->byteOrder == SB_MSB ? 1 : 0};
+    for (size_t k = 0; k < (size_t)f->nr * f->na; k++) memcpy(buf + 4 * k, one, 4);
+    const char *src = v.nbands > 0 ? v.source : intFile;
+    FILE *fp = fopen(src, "rb");
+    if (!fp) sbio_die("getInt: cannot open %s", src);
+    fseeko(fp, 0, SEEK_END);
+    off_t size = ftello(fp);
+    fseeko(fp, 0, SEEK_SET);
+    size_t nLines = (size_t)size / row;
+    if (nLines > (size_t)f->na) nLines = f->na;
+    if (nLines && fread(buf, row, nLines, fp) != nLines) sbio_die("getInt: short read on %s", src);
+    fclose(fp);
+    f->data = buf;
+}
+
 static void *load_image(const char *image, const char *parKey, const sbio_rdf *r, const Args *a, sb_image *im,
                         int *vrtByteOrder)
 {
@@ -191,8 +238,15 @@ int main(int argc, char **argv)
     im1.byteOrder = im2.byteOrder = a.floatFlag ? byteOrder : SB_MSB;
 
     /* ---- interferogram, geodat, baseline (strack.c:92-126) */
-    if (sbio_rdf_get(r, "intfile"))
-        sbio_die("intfile: interferogram-aided phase correction (getInt/phaseCorrectInt) is not supported");
+    sb_interferogram intf;
+    memset(&intf, 0, sizeof intf);
+#ifndef STRACKW
+    const char *intFile = sbio_rdf_get(r, "intfile");
+    if (intFile && !a.noComplex) {
+        load_interferogram(intFile, &intf);
+        p.intf = &intf;
+    }
+#endif
     const char *intGeodat = sbio_rdf_get(r, "intgeodat");
 #ifndef STRACKW
     if (!intGeodat) sbio_die("getInt: Missing geodat filename");

@@ -140,3 +140,32 @@ def test_strackw_and_cullst_cli(tools, tmp_path, pair):
     assert np.array_equal(files.read_grid(str(tmp_path / "culled.da"), nR, nA), d["offAS"])
     assert np.array_equal(files.read_grid(str(tmp_path / "in.sr"), nR, nA), d["sigmaR"])
     assert os.path.exists(tmp_path / "culled.vrt") and os.path.exists(tmp_path / "culled.mt.vrt")
+
+
+@pytest.mark.gpu
+def test_strack_cli_interferogram(tools, tmp_path):
+    """intfile: the interferogram (big-endian CInt16 with looks in its VRT)
+    flattens the fringe exactly as the library call does; a short file's
+    missing lines hold (1, 1) like getInt's fill."""
+    import torch
+    from specklesource_b200 import runtime
+    s1, s2 = synth.make_pair(256, 512, 11, dr=lambda y, x: 1.3 + 0 * x, da=lambda y, x: 0.4 + 0 * x,
+                             coherence=0.8, ramp=0.6)
+    a, b = synth.to_numpy(s1), synth.to_numpy(s2)
+    kv = _setup_track(tmp_path, a, b, rstart=40, astart=40, deltar=16, deltaa=16, nR=27, nA=12)
+    intf = synth.fringe_interferogram(256, 512, 4, 2, 0.6)
+    files.write_interferogram(str(tmp_path / "int.int"), intf, 4, 2, lines=100)
+    with open(tmp_path / "track.par", "a") as f:
+        f.write("intfile = int.int\n")
+    r = _run(tools["strack"], ["track.par"], tmp_path)
+    assert r.returncode == 0, r.stderr
+    out = files.read_track_outputs(str(tmp_path / "out"), kv["nR"], kv["nA"])
+    full = intf.copy()
+    full[100:] = np.array([1, 1], ">i2")
+    p = abi.TrackParams(rStart=40, aStart=40, deltaR=16, deltaA=16, nR=27, nA=12, wR=32, wA=32, wRa=32, wAa=32,
+                        intf=dict(data=full, nrl=4, nal=2))
+    with runtime.Context(0) as ctx:
+        g = ctx.strack(p, a, b)
+    for k, q in (("dr", "offR"), ("da", "offA"), ("mt", "type")):
+        assert np.array_equal(out[k], g[q]), k
+    assert (g["type"][:6] == 1).all()  # rows whose interferogram patches lie in the file's 100 lines
