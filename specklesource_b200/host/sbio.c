@@ -209,6 +209,17 @@ int sbio_vrt_read(const char *path, sbio_vrt *v)
         v->byteOrder = strcasecmp(buf, "MSB") == 0 ? SB_MSB : SB_LSB;
     for (const char *b = band; b && v->nbands < 8; b = strcasestr(b + 1, "<VRTRasterBand")) {
         if (!element(b, "SourceFilename", buf, sizeof buf)) continue;
+        /* per-band facts, looked up only inside this band's element */
+        const char *end = strcasestr(b, "</VRTRasterBand>");
+        size_t blen = end ? (size_t)(end - b) : strlen(b);
+        char *bb = strndup(b, blen);
+        char tmp[256];
+        const int k = v->nbands;
+        v->desc[k][0] = '\0';
+        if (element(bb, "Description", tmp, sizeof tmp)) snprintf(v->desc[k], 256, "%s", tmp);
+        v->bandMSB[k] = element(bb, "ByteOrder", tmp, sizeof tmp) && strcasecmp(tmp, "MSB") == 0;
+        v->offset[k] = element(bb, "ImageOffset", tmp, sizeof tmp) ? atoll(tmp) : 0;
+        free(bb);
         const char *tag = strcasestr(b, "<SourceFilename");
         char rel[16] = "";
         attr(tag, "relativeToVRT", rel, sizeof rel);
@@ -235,6 +246,20 @@ int sbio_vrt_read(const char *path, sbio_vrt *v)
     }
     free(txt);
     return 1;
+}
+
+float *sbio_vrt_read_float_band(const sbio_vrt *v, int b, size_t n)
+{
+    if (b < 0 || b >= v->nbands) sbio_die("VRT has no band %d", b + 1);
+    size_t sz;
+    unsigned char *all = sbio_read_all(v->sources[b], &sz);
+    const size_t off = (size_t)v->offset[b];
+    if (sz < off + n * 4) sbio_die("%s holds %zu bytes, band needs %zu", v->sources[b], sz, off + n * 4);
+    float *out = malloc(n * sizeof(float));
+    memcpy(out, all + off, n * sizeof(float));
+    free(all);
+    if (v->bandMSB[b]) swap_items((unsigned char *)out, 4, n);
+    return out;
 }
 
 const char *sbio_vrt_meta(const sbio_vrt *v, const char *key)

@@ -38,11 +38,17 @@ typedef struct {
     int sampleType;     /* SB_CFLOAT32, SB_CINT16, or -1 (Float32/Byte bands) */
     char source[4096];  /* path of band 1's raw file (resolved relative to the VRT) */
     char sources[8][4096]; /* every band's raw file, resolved the same way */
+    char desc[8][256];     /* every band's <Description> ("" when absent) */
+    int bandMSB[8];        /* every band's ByteOrder (1: MSB; 0: LSB or not stated) */
+    long long offset[8];   /* every band's ImageOffset in bytes */
     int nbands;
     char meta[64][2][256];
     int nmeta;
 } sbio_vrt;
 int sbio_vrt_read(const char *path, sbio_vrt *v);
+/* Reads band b (float32) of a VRT into n floats, honouring its byte order and
+ * image offset. */
+float *sbio_vrt_read_float_band(const sbio_vrt *v, int b, size_t n);
 const char *sbio_vrt_meta(const sbio_vrt *v, const char *key);
 
 typedef struct {

@@ -269,7 +269,28 @@ int main(int argc, char **argv)
     /* ---- initial offsets (parseInitialOffsets.c, readBothOffsetsStrack.c) */
     sb_offset_grid grid;
     const char *initShift = sbio_rdf_get(r, "initShift");
-    if (initShift) {
+    char *initVrt = initShift ? suffixed(initShift, ".vrt") : NULL;
+    if (initShift && sbio_exists(initVrt)) {
+        /* readBothOffsetsStrackVrt (Strack/readBothOffsetsStrack.c:46-77): band 1
+           the range offsets, band 2 the azimuth offsets, r0/a0/deltaR/deltaA metadata */
+        p.polyShift = 0;
+        sbio_vrt v;
+        if (!sbio_vrt_read(initVrt, &v) || v.nbands < 2) sbio_die("Problem reading offsets from %s", initVrt);
+        const char *m0 = sbio_vrt_meta(&v, "r0"), *m1 = sbio_vrt_meta(&v, "a0");
+        const char *m2 = sbio_vrt_meta(&v, "deltaR"), *m3 = sbio_vrt_meta(&v, "deltaA");
+        if (!m0 || !m1 || !m2 || !m3) sbio_die("%s lacks r0/a0/deltaR/deltaA", initVrt);
+        if (!strstr(v.desc[0], "Range")) sbio_die("Problem reading range offsets from %s", initVrt);
+        if (!strstr(v.desc[1], "Azimuth")) sbio_die("Problem reading azimuth offsets from %s", initVrt);
+        grid.nr = v.nr;
+        grid.na = v.na;
+        grid.r0 = atoi(m0);
+        grid.a0 = atoi(m1);
+        grid.deltaR = (float)atof(m2);
+        grid.deltaA = (float)atof(m3);
+        grid.dr = sbio_vrt_read_float_band(&v, 0, (size_t)grid.nr * grid.na);
+        grid.da = sbio_vrt_read_float_band(&v, 1, (size_t)grid.nr * grid.na);
+        p.initOffsets = &grid;
+    } else if (initShift) {
         p.polyShift = 0;
         double h[6];
         char *daFile = suffixed(initShift, ".da"), *drFile = suffixed(initShift, ".dr");

@@ -169,3 +169,28 @@ def test_strack_cli_interferogram(tools, tmp_path):
     for k, q in (("dr", "offR"), ("da", "offA"), ("mt", "type")):
         assert np.array_equal(out[k], g[q]), k
     assert (g["type"][:6] == 1).all()  # rows whose interferogram patches lie in the file's 100 lines
+
+
+@pytest.mark.gpu
+def test_initial_offsets_from_vrt_or_dat(tools, tmp_path, pair):
+    """initShift: the offsets VRT (range and azimuth bands with r0/a0/deltaR/
+    deltaA metadata, readBothOffsetsStrackVrt) and the .da/.dr/.dat files
+    (readBothOffsetsStrack) give the same run."""
+    a, b = pair
+    _setup_track(tmp_path, a, b, outputfile="prev")
+    r = _run(tools["strack"], ["track.par"], tmp_path)
+    assert r.returncode == 0, r.stderr
+    txt = (tmp_path / "track.par").read_text().replace("outputfile = prev", "outputfile = out")
+    (tmp_path / "track.par").write_text(txt + "initShift = prev\n")
+    r = _run(tools["strack"], ["track.par"], tmp_path)
+    assert r.returncode == 0, r.stderr
+    via_vrt = files.read_track_outputs(str(tmp_path / "out"), 27, 25)
+    os.remove(tmp_path / "prev.vrt")
+    # the older route reads <initShift>.da.dat, as readBothOffsetsStrack does
+    (tmp_path / "prev.da.dat").write_text((tmp_path / "prev.dat").read_text())
+    r = _run(tools["strack"], ["track.par"], tmp_path)
+    assert r.returncode == 0, r.stderr
+    via_dat = files.read_track_outputs(str(tmp_path / "out"), 27, 25)
+    for k in ("dr", "da", "mt"):
+        assert np.array_equal(via_vrt[k], via_dat[k]), k
+    assert (via_vrt["mt"] > 0).mean() > 0.9
