@@ -166,7 +166,7 @@ typedef struct {
     int32_t hanningFlag;    /* 1 unless -noHanning */
     int32_t maxTries;       /* 2, or 1 with -singleAmp */
     int32_t checkAzFocus;   /* -checkAzFocus */
-    int32_t gaussFlag;      /* -gauss: experimental 2-D fit, not supported */
+    int32_t gaussFlag;      /* -gauss: 2-D Gaussian peak fit (cmpTrackGauss) */
     float azDefocusThresh;  /* 1.8 in the reference CLI */
     /* strackw parameters (parseTrack.c:222-253) */
     int32_t edgePadR, edgePadA; /* search radius, before the internal +NFAST/4 */

@@ -481,6 +481,165 @@ static void gaussPeak1D(const FLT *cMag, int ncol, int iMax, int jMax, int AzOrR
     *peakRatio = a[1];
 }
 
+/* ---------------------------------------------------------------- 2-D fit (-gauss) */
+
+/* Gauss-Jordan with full pivoting for the 5 x 5 system of the 2-D fit (the
+ * same Numerical Recipes algorithm as gaussj3). */
+static int gaussj5(FLT a[6][6], int n, FLT b[6])
+{
+    int indxc[6], indxr[6], ipiv[6] = {0, 0, 0, 0, 0, 0};
+    int irow = 0, icol = 0;
+    for (int i = 1; i <= n; i++) {
+        FLT big = 0.0;
+        for (int j = 1; j <= n; j++)
+            if (ipiv[j] != 1)
+                for (int k = 1; k <= n; k++) {
+                    if (ipiv[k] == 0) {
+                        if (fabs((double)a[j][k]) >= big) {
+                            big = (FLT)fabs((double)a[j][k]);
+                            irow = j;
+                            icol = k;
+                        }
+                    } else if (ipiv[k] > 1)
+                        return 0;
+                }
+        ++(ipiv[icol]);
+        if (irow != icol) {
+            for (int l = 1; l <= n; l++) { FLT t = a[irow][l]; a[irow][l] = a[icol][l]; a[icol][l] = t; }
+            FLT t = b[irow]; b[irow] = b[icol]; b[icol] = t;
+        }
+        indxr[i] = irow;
+        indxc[i] = icol;
+        if (a[icol][icol] == 0.0) return 0;
+        FLT pivinv = (FLT)(1.0 / a[icol][icol]);
+        a[icol][icol] = 1.0;
+        for (int l = 1; l <= n; l++) a[icol][l] *= pivinv;
+        b[icol] *= pivinv;
+        for (int ll = 1; ll <= n; ll++)
+            if (ll != icol) {
+                FLT dum = a[ll][icol];
+                a[ll][icol] = 0.0;
+                for (int l = 1; l <= n; l++) a[ll][l] -= a[icol][l] * dum;
+                b[ll] -= b[icol] * dum;
+            }
+    }
+    (void)indxc;
+    (void)indxr;
+    return 1;
+}
+
+/* myGauss, speckleTrack.c:2421-2443: amplitude, mux, sigx, muy, sigy */
+static void myGauss2D(FLT px, FLT py, const FLT a[6], FLT *y, FLT dyda[6])
+{
+    FLT dx = px - a[2], dy = py - a[4];
+    FLT argx = (FLT)0.5 * (dx * dx) / (a[3] * a[3]);
+    FLT argy = (FLT)0.5 * (dy * dy) / (a[5] * a[5]);
+    FLT ex = (FLT)exp((double)(-argx - argy));
+    *y = a[1] * ex;
+    dyda[1] = ex;
+    dyda[2] = (*y) * (px - a[2]) / (a[3] * a[3]);
+    dyda[3] = *y * (px - a[2]) * (px - a[2]) / (a[3] * a[3] * a[3]);
+    dyda[4] = *y * (py - a[4]) / (a[5] * a[5]);
+    dyda[5] = *y * (py - a[4]) * (py - a[4]) / (a[5] * a[5] * a[5]);
+}
+
+static void mrqcof2D(const FLT *px, const FLT *py, const FLT *z, int n, const FLT a[6], FLT alpha[6][6], FLT beta[6],
+                     FLT *chisq)
+{
+    /* mrqcofMod with ma = mfit = 5, sig = 1 */
+    FLT ymod, dyda[6];
+    for (int j = 1; j <= 5; j++) {
+        for (int k = 1; k <= j; k++) alpha[j][k] = 0.0;
+        beta[j] = 0.0;
+    }
+    *chisq = 0.0;
+    for (int i = 1; i <= n; i++) {
+        myGauss2D(px[i], py[i], a, &ymod, dyda);
+        FLT dy = z[i] - ymod;
+        for (int l = 1; l <= 5; l++) {
+            FLT wt = dyda[l];
+            for (int m = 1; m <= l; m++) alpha[l][m] += wt * dyda[m];
+            beta[l] += dy * wt;
+        }
+        *chisq += dy * dy;
+    }
+    for (int j = 2; j <= 5; j++)
+        for (int k = 1; k < j; k++) alpha[k][j] = alpha[j][k];
+}
+
+/* cmpTrackGauss, speckleTrack.c:2205-2303: 18 x 18 samples of |c| around the
+ * coarse peak, scaled to correlation units, a 2-D Gaussian by <= 8 LM steps
+ * (stop when both centres move < 0.001); peak in NOVER units of the 2x grid. */
+static void cmpTrackGauss(StCtx *c, int *iMax, int *jMax, double *cMax, int wR, int wA, const FLT *cFunc, double p1,
+                          double p2, int isComplex)
+{
+    const int nG = NGAUSS;
+    if ((*iMax - nG / 2) < 0 || (*iMax + nG / 2) >= (wA * OS - 1) || (*jMax - nG / 2) < 0 ||
+        (*jMax + nG / 2) >= (wR * OS - 1)) {
+        *iMax = -LARGEINT;
+        *jMax = -LARGEINT;
+        *cMax = 0;
+        return;
+    }
+    FLT px[NGAUSS * NGAUSS + 1], py[NGAUSS * NGAUSS + 1], z[NGAUSS * NGAUSS + 1];
+    const double hc = (c->p->hanningFlag == TRUE && isComplex == TRUE) ? 1.5 : 1.0;
+    const double scale = hc / (sqrt(p1 * p2) * pow((double)(wR * wA), 2));
+    int iData = 1;
+    for (int i = 0; i < nG; i++) {
+        int i1 = *iMax - nG / 2 + i, j1 = *jMax - nG / 2;
+        for (int j = 0; j < nG; j++) {
+            px[iData] = (FLT)i1;
+            py[iData] = (FLT)j1;
+            z[iData] = (FLT)(cFunc[i1 * wR * OSA + j1] * scale);
+            iData++;
+            j1++;
+        }
+    }
+    FLT a[6] = {0, (FLT)(*cMax * scale), (FLT)*iMax, 3, (FLT)*jMax, 3};
+    FLT alpha[6][6], beta[6], chisq = 0, ochisq = 0, alamda = -1;
+    FLT lasti = (FLT)2e9, lastj = (FLT)2e9;
+    for (int it = 0; it < 8; it++) {
+        FLT covar[6][6], da[6], atry[6];
+        if (alamda < 0.0) {
+            alamda = (FLT)0.001;
+            mrqcof2D(px, py, z, iData - 1, a, alpha, beta, &chisq);
+            ochisq = chisq;
+        }
+        for (int j = 1; j <= 5; j++) {
+            for (int k = 1; k <= 5; k++) covar[j][k] = alpha[j][k];
+            covar[j][j] = alpha[j][j] * (FLT)(1.0 + alamda);
+            da[j] = beta[j];
+        }
+        if (!gaussj5(covar, 5, da)) break; /* Numerical Recipes would exit: the fit ends */
+        for (int l = 1; l <= 5; l++) atry[l] = a[l] + da[l];
+        atry[0] = a[0];
+        mrqcof2D(px, py, z, iData - 1, atry, covar, da, &chisq);
+        if (chisq < ochisq) {
+            alamda *= (FLT)0.1;
+            ochisq = chisq;
+            for (int j = 1; j <= 5; j++) {
+                for (int k = 1; k <= 5; k++) alpha[j][k] = covar[j][k];
+                beta[j] = da[j];
+            }
+            for (int l = 1; l <= 5; l++) a[l] = atry[l];
+        } else {
+            alamda *= (FLT)10.0;
+            chisq = ochisq;
+        }
+        if (fabs((double)(a[2] - lasti)) < 0.001 && fabs((double)(a[4] - lastj)) < 0.001) break;
+        lasti = a[2];
+        lastj = a[4];
+    }
+    *iMax = (int)round((double)(a[2] * NOVER)); /* float product, as the reference's float a[] */
+    *jMax = (int)round((double)(a[4] * NOVER));
+    *cMax = a[1] < 1.0 ? a[1] : 1.0;
+    if ((0.5 * a[3]) > 1000.0 || (0.5 * a[5]) > 1000.0) {
+        *iMax = -LARGEINT;
+        *jMax = -LARGEINT;
+        *cMax = 0;
+    }
+}
+
 /* ---------------------------------------------------------------- peaks */
 
 /* findCPeak, speckleTrack.c:744-805: fftshift |c| into corrF while taking the
@@ -762,7 +921,13 @@ static int complexMatch(StCtx *c, int r1, int a1, int *iMax, int *jMax, double *
     phaseCorrectBaseline(c, r1, a1);
     phaseCorrectInt(c, r1, a1);
     cmpPSWithPad(c);
-    cmpTrackFast(c, iMax, jMax, cMax);
+    if (c->p->gaussFlag == TRUE) {
+        /* speckleTrack.c:366-371 */
+        offt2d_exec(c->cReverseNoPad, c->psNoPad, c->cNoPad);
+        findCPeak(c->cNoPadMag, c->cNoPad, c->wR * OS, c->wA * OS, iMax, jMax, cMax);
+        cmpTrackGauss(c, iMax, jMax, cMax, c->wR, c->wA, c->cNoPadMag, c->p1, c->p2, TRUE);
+    } else
+        cmpTrackFast(c, iMax, jMax, cMax);
     good = FALSE;
     int iM = *iMax / NOVER; /* lround of an integer quotient */
     int jM = *jMax / NOVER;
@@ -838,6 +1003,11 @@ static void ampTrackFast(StCtx *c, int *iMax, int *jMax, double *cMax, double p1
     }
     if (*iMax < -999 || (fabs(c->aZDefocus[outIdx]) >= c->p->azDefocusThresh && c->p->checkAzFocus == TRUE))
         return;
+    if (c->p->gaussFlag == TRUE) {
+        /* speckleTrack.c:551-557: pScale 16 matches the complex normalisation */
+        cmpTrackGauss(c, iMax, jMax, cMax, wR, wA, b->caMag, p1 * 16., p2 * 16., FALSE);
+        return;
+    }
     int iMax1, jMax1;
     *cMax = overSamplePeak(c, b->caMag, wR * OSA, *iMax, *jMax, &iMax1, &jMax1);
     *cMax = *cMax / (pow((double)(wA * OS), 2) * pow((double)(wR * OS), 2) * pow((double)NFAST, 2));
@@ -907,7 +1077,6 @@ int oracle_strack(const sb_track_params *p, const sb_image *img1, const sb_image
                   int32_t row0, int32_t row1)
 {
     if (!p || !img1 || !img2 || !out) return SB_ERR_ARG;
-    if (p->gaussFlag) return SB_ERR_UNSUPPORTED;
     if (p->hanningFlag && p->wR != p->wA) return SB_ERR_UNSUPPORTED;
     if (p->polyShift == 0 && p->initOffsets == NULL) return SB_ERR_ARG;
     if (p->intf && (p->intf->nal <= 0 || p->intf->nrl <= 0 || p->intf->nr <= 0 || p->intf->na <= 0 ||

@@ -491,7 +491,6 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
     if (p->nR <= 0 || p->nA <= 0) return sb_ctx_fail(c, SB_ERR_ARG, "empty grid nR=%d nA=%d", p->nR, p->nA);
     if ((int64_t)p->nR * p->nA > (int64_t)1 << 30) return sb_ctx_fail(c, SB_ERR_ARG, "grid too large");
     if (p->scaleFactor <= 0) return sb_ctx_fail(c, SB_ERR_ARG, "scaleFactor must be positive");
-    if (p->gaussFlag) return sb_ctx_fail(c, SB_ERR_UNSUPPORTED, "-gauss (experimental 2-D fit) is not supported");
     if (p->polyShift == 0 && !p->initOffsets) return sb_ctx_fail(c, SB_ERR_ARG, "polyShift=0 needs initOffsets");
     if (p->mask && (p->mask->nal <= 0 || p->mask->nrl <= 0 || !p->mask->mask))
         return sb_ctx_fail(c, SB_ERR_ARG, "invalid mask");
@@ -636,6 +635,7 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
         a.tau = tau_table(c, W);
         a.osA = osA_table(c);
         a.osD = osD_table(c);
+        a.gauss = p->gaussFlag ? 1 : 0;
         a.azThresh = p->azDefocusThresh;
         a.checkAzFocus = p->checkAzFocus;
         a.noComplex = p->noComplex;
@@ -764,6 +764,7 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
         a.tau = tau_table(c, Ws);
         a.osA = osA_table(c);
         a.osD = osD_table(c);
+        a.gauss = p->gaussFlag ? 1 : 0;
         a.rec = drec;
         a.fit = dfit;
         // small windows: everything in shared memory; larger: per-CTA

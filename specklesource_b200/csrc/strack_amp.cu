@@ -36,7 +36,7 @@ struct AmpCfg {
     static constexpr size_t scratch = (size_t)3 * WS * WS + (size_t)N * N + (size_t)N * N / 2;
 };
 
-template <int WS>
+template <int WS, bool GAUSS>
 __global__ void __launch_bounds__(AmpCfg<WS>::NT, 2) strack_amp_kernel(AmpArgs a)
 {
     using C = AmpCfg<WS>;
@@ -263,7 +263,15 @@ __global__ void __launch_bounds__(AmpCfg<WS>::NT, 2) strack_amp_kernel(AmpArgs a
         }
         const double cRaw = cMax;
         const int iC = iMax, jC = jMax;
-        if (iMax >= -999) {
+        if (GAUSS && iMax >= -999) {
+            // -gauss: cmpTrackGauss on the amplitude plane (:553-557; pScale
+            // 16, no hanning correction), unless the fit kernel takes the
+            // early return of ampTrackFast
+            const double hw = (double)(N / 2) * (double)(N / 2);
+            const double scale = 1.0 / (sqrt((p1 * 16.0) * (p2 * 16.0)) * pow(hw, 2));
+            gauss2d_peak<NT>([=](int i, int j) { return mag[i * N + j]; }, N, scale, reinterpret_cast<float*>(T), blk, iMax,
+                             jMax, cMax);
+        } else if (iMax >= -999) {
             // 8x8 -> 96x96 oversampling (used unless the fit kernel takes the
             // early return of ampTrackFast, :551-553)
             if (tid < NFAST * NFAST) {
@@ -298,15 +306,21 @@ __global__ void __launch_bounds__(AmpCfg<WS>::NT, 2) strack_amp_kernel(AmpArgs a
     }
 }
 
+template <int WS, bool GAUSS>
+static cudaError_t launch_amp_t(const AmpArgs& a, int nCta, cudaStream_t st)
+{
+    using C = AmpCfg<WS>;
+    cudaError_t e = cudaFuncSetAttribute(strack_amp_kernel<WS, GAUSS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)C::smem);
+    if (e != cudaSuccess) return e;
+    strack_amp_kernel<WS, GAUSS><<<nCta, C::NT, C::smem, st>>>(a);
+    return cudaGetLastError();
+}
+
 template <int WS>
 static cudaError_t launch_amp(const AmpArgs& a, int nCta, cudaStream_t st)
 {
-    using C = AmpCfg<WS>;
-    cudaError_t e =
-        cudaFuncSetAttribute(strack_amp_kernel<WS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem);
-    if (e != cudaSuccess) return e;
-    strack_amp_kernel<WS><<<nCta, C::NT, C::smem, st>>>(a);
-    return cudaGetLastError();
+    return a.gauss ? launch_amp_t<WS, true>(a, nCta, st) : launch_amp_t<WS, false>(a, nCta, st);
 }
 
 bool amp_supported(int Ws)

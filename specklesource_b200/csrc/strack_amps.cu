@@ -81,7 +81,7 @@ __device__ __forceinline__ int cpeak_plane(const float* mag, float pmax, unsigne
     return y * N + x;
 }
 
-template <int WS, int NT>
+template <int WS, int NT, bool GAUSS>
 __global__ void __launch_bounds__(NT, (WS == 32 ? 3 : 2)) strack_amps_kernel(AmpArgs a)
 {
     using M = AmpsSmem<WS, NT>;
@@ -313,7 +313,15 @@ __global__ void __launch_bounds__(NT, (WS == 32 ? 3 : 2)) strack_amps_kernel(Amp
         }
         const double cRaw = cMax;
         const int iC = iMax, jC = jMax;
-        if (iMax >= -999) {
+        if (GAUSS && iMax >= -999) {
+            // -gauss: cmpTrackGauss on the amplitude plane (:553-557; pScale
+            // 16, no hanning correction), unless the fit kernel takes the
+            // early return of ampTrackFast
+            const double hw = (double)(N / 2) * (double)(N / 2);
+            const double scale = 1.0 / (sqrt((p1 * 16.0) * (p2 * 16.0)) * pow(hw, 2));
+            gauss2d_peak<NT>([=](int i, int j) { return sqrtf(zf[i * N + j]); }, N, scale, reinterpret_cast<float*>(T), blk, iMax,
+                             jMax, cMax);
+        } else if (iMax >= -999) {
             // 8x8 -> 96x96 oversampling (used unless the fit kernel takes the
             // early return of ampTrackFast, :551-553)
             if (tid < NFAST * NFAST) {
@@ -348,15 +356,21 @@ __global__ void __launch_bounds__(NT, (WS == 32 ? 3 : 2)) strack_amps_kernel(Amp
     }
 }
 
+template <int WS, int NT, bool GAUSS>
+static cudaError_t launch_amps_t(const AmpArgs& a, int nCta, cudaStream_t st)
+{
+    const size_t sm = AmpsSmem<WS, NT>::bytes;
+    cudaError_t e = cudaFuncSetAttribute(strack_amps_kernel<WS, NT, GAUSS>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    strack_amps_kernel<WS, NT, GAUSS><<<nCta, NT, sm, st>>>(a);
+    return cudaGetLastError();
+}
+
 template <int WS, int NT>
 static cudaError_t launch_amps(const AmpArgs& a, int nCta, cudaStream_t st)
 {
-    const size_t sm = AmpsSmem<WS, NT>::bytes;
-    cudaError_t e =
-        cudaFuncSetAttribute(strack_amps_kernel<WS, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return e;
-    strack_amps_kernel<WS, NT><<<nCta, NT, sm, st>>>(a);
-    return cudaGetLastError();
+    return a.gauss ? launch_amps_t<WS, NT, true>(a, nCta, st) : launch_amps_t<WS, NT, false>(a, nCta, st);
 }
 
 template <int WS, int NT>
@@ -364,8 +378,8 @@ static int occupancy_amps()
 {
     int nb = 0;
     const size_t sm = AmpsSmem<WS, NT>::bytes;
-    cudaFuncSetAttribute(strack_amps_kernel<WS, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, strack_amps_kernel<WS, NT>, NT, sm);
+    cudaFuncSetAttribute(strack_amps_kernel<WS, NT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, strack_amps_kernel<WS, NT, false>, NT, sm);
     return nb;
 }
 

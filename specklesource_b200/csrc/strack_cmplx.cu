@@ -281,7 +281,7 @@ __device__ __forceinline__ void phase_correct_int(const CmplxArgs& a, const Poin
     __syncthreads();
 }
 
-template <int W, int NT, bool F32>
+template <int W, int NT, bool F32, bool GAUSS>
 __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(CmplxArgs a)
 {
     using S = CmplxSmem<W, NT>;
@@ -451,12 +451,37 @@ __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(Cmp
         double cMax;
         const bool rejected = (iMax < (NFAST / 2) || iMax > (W2 - NFAST / 2) || jMax < (NFAST / 2) ||
                                jMax > (W2 - NFAST / 2));
-        int gate = 0;
         if (rejected) {
             cMax = -1.0;
             iMax = -1000;
             jMax = -1000;
-        } else {
+        }
+        // samples for gaussPeak1D x 2 through the peak (NOVER units in)
+        auto fit_samples = [&](int iMx, int jMx) -> int {
+            const int iM = iMx / NOVER, jM = jMx / NOVER;
+            const int g =
+                (iM - NGAUSS / 2) >= 0 && (iM + NGAUSS / 2) < W2 && (jM - NGAUSS / 2) >= 0 && (jM + NGAUSS / 2) < W2;
+            if (g && tid < 2 * NGAUSS) {
+                const int f = tid / NGAUSS, k = tid % NGAUSS;
+                FitJob* fj = &a.fit[it];
+                if (f == 0) {
+                    fj->samp[0][k] = sqrtf(fmap<W>(smf, iM, jM - NGAUSS / 2 + k));
+                } else {
+                    fj->samp[1][k] = sqrtf(fmap<W>(smf, iM - NGAUSS / 2 + k, jM));
+                }
+                if (k == 0) fj->x0[f] = (f == 0 ? jM : iM) - NGAUSS / 2;
+            }
+            return g;
+        };
+        int gate = 0;
+        if constexpr (GAUSS) {
+            // cmpTrackGauss on the 2x grid (hanning correction as the oversampling's)
+            const double scale = a.hanCorr / (sqrt(p1 * p2) * pow((double)(W * W), 2));
+            if (!rejected) cMax = (double)sqrtf(fmap<W>(smf, iMax, jMax));
+            gauss2d_peak<NT>([smf](int i, int j) { return sqrtf(fmap<W>(smf, i, j)); }, W2, scale,
+                             reinterpret_cast<float*>(T), blk, iMax, jMax, cMax);
+            gate = fit_samples(iMax, jMax);
+        } else if (!rejected) {
             // ------------------------------------------------ overSampleC on the 8x8 block
             if (tid < NFAST * NFAST) {
                 const int t1 = tid / NFAST, t2 = tid % NFAST;
@@ -470,20 +495,7 @@ __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(Cmp
             cMax = a.hanCorr * cMax / (sqrt(p1 * p2) * pow((double)(W * W), 2));
             iMax = (iMax * NOVER) + iMax1 - (NOVER * NFAST) / 2;
             jMax = (jMax * NOVER) + jMax1 - (NOVER * NFAST) / 2;
-            // ------------------------------------------------ samples for gaussPeak1D x 2
-            const int iM = iMax / NOVER, jM = jMax / NOVER;
-            gate = (iM - NGAUSS / 2) >= 0 && (iM + NGAUSS / 2) < W2 && (jM - NGAUSS / 2) >= 0 &&
-                   (jM + NGAUSS / 2) < W2;
-            if (gate && tid < 2 * NGAUSS) {
-                const int f = tid / NGAUSS, k = tid % NGAUSS;
-                FitJob* fj = &a.fit[it];
-                if (f == 0) {
-                    fj->samp[0][k] = sqrtf(fmap<W>(smf, iM, jM - NGAUSS / 2 + k));
-                } else {
-                    fj->samp[1][k] = sqrtf(fmap<W>(smf, iM - NGAUSS / 2 + k, jM));
-                }
-                if (k == 0) fj->x0[f] = (f == 0 ? jM : iM) - NGAUSS / 2;
-            }
+            gate = fit_samples(iMax, jMax);
         }
         if (tid == 0) {
             PointRec* r = &a.rec[p];
@@ -500,22 +512,24 @@ __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(Cmp
     }
 }
 
-template <int W, int NT, bool F32>
+template <int W, int NT, bool F32, bool GAUSS>
 static cudaError_t launch_cmplx_t(const CmplxArgs& a, int nCta, cudaStream_t st)
 {
     const size_t sm = CmplxSmem<W, NT>::bytes;
-    cudaError_t e = cudaFuncSetAttribute(strack_cmplx_kernel<W, NT, F32>,
+    cudaError_t e = cudaFuncSetAttribute(strack_cmplx_kernel<W, NT, F32, GAUSS>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    strack_cmplx_kernel<W, NT, F32><<<nCta, NT, sm, st>>>(a);
+    strack_cmplx_kernel<W, NT, F32, GAUSS><<<nCta, NT, sm, st>>>(a);
     return cudaGetLastError();
 }
 
 template <int W, int NT>
 static cudaError_t launch_cmplx(const CmplxArgs& a, int nCta, cudaStream_t st)
 {
-    return a.sampleType == SB_CFLOAT32 ? launch_cmplx_t<W, NT, true>(a, nCta, st)
-                                       : launch_cmplx_t<W, NT, false>(a, nCta, st);
+    const bool f32 = a.sampleType == SB_CFLOAT32;
+    if (a.gauss)
+        return f32 ? launch_cmplx_t<W, NT, true, true>(a, nCta, st) : launch_cmplx_t<W, NT, false, true>(a, nCta, st);
+    return f32 ? launch_cmplx_t<W, NT, true, false>(a, nCta, st) : launch_cmplx_t<W, NT, false, false>(a, nCta, st);
 }
 
 template <int W, int NT>
@@ -523,8 +537,9 @@ static int occupancy_cmplx()
 {
     int nb = 0;
     const size_t sm = CmplxSmem<W, NT>::bytes;
-    cudaFuncSetAttribute(strack_cmplx_kernel<W, NT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, strack_cmplx_kernel<W, NT, true>, NT, sm);
+    cudaFuncSetAttribute(strack_cmplx_kernel<W, NT, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sm);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, strack_cmplx_kernel<W, NT, true, false>, NT, sm);
     return nb;
 }
 

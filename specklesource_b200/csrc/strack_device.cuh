@@ -1,6 +1,7 @@
 // strack_device.cuh -- device helpers shared by the strack stage kernels:
 // block reductions, the fftshift argmax of findCPeak, the 8x8 -> 96x96
-// oversampling window, and the Levenberg-Marquardt 1-D Gaussian peak fit.
+// oversampling window, the Levenberg-Marquardt 1-D Gaussian peak fit and
+// the 2-D Gaussian peak fit of the -gauss mode.
 #pragma once
 #include <cuda_runtime.h>
 #include <math.h>
@@ -447,6 +448,189 @@ __device__ __forceinline__ int dop_shift(double sr1, double si1, double sr2, dou
     int shift = (v != v) ? 0 : ((v >= 0.0) ? (int)(v + 0.5) : (int)(v - 0.5));
     if (shift < 0) shift += nAz;
     return (int)((float)shift * (float)wA / (float)nAz);
+}
+
+// cmpTrackGauss (Strack/speckleTrack.c:2205-2303, the -gauss mode): a 2-D
+// Gaussian (amplitude, centre and width per axis; myGauss :2421-2443) fitted
+// to the 18 x 18 samples S of |c| * scale around the coarse peak by the
+// Levenberg-Marquardt steps of mrqminMod (:2353-2416) in float, <= 8 steps,
+// stopping when both centres move < 0.001.  Run by one warp: per-sample terms
+// on the lanes, the 5 x 5 Gauss-Jordan solve (full pivoting) on every lane.
+static __device__ __forceinline__ void lm2d_cof(const float* S, float i0, float j0, const float (&a)[6], float (&al)[6][6],
+                                         float (&be)[6], float& chisq)
+{
+    const int lane = threadIdx.x & 31;
+    float A[15], B[5], c2 = 0.f;
+#pragma unroll
+    for (int k = 0; k < 15; ++k) A[k] = 0.f;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) B[k] = 0.f;
+    for (int k = lane; k < NGAUSS * NGAUSS; k += 32) {
+        const float px = i0 + (float)(k / NGAUSS), py = j0 + (float)(k % NGAUSS);
+        const float dx = px - a[2], dyv = py - a[4];
+        const float argx = 0.5f * (dx * dx) / (a[3] * a[3]);
+        const float argy = 0.5f * (dyv * dyv) / (a[5] * a[5]);
+        const float ex = expf(-argx - argy);
+        const float y = a[1] * ex;
+        const float d[5] = {ex, y * (px - a[2]) / (a[3] * a[3]), y * (px - a[2]) * (px - a[2]) / (a[3] * a[3] * a[3]),
+                            y * (py - a[4]) / (a[5] * a[5]), y * (py - a[4]) * (py - a[4]) / (a[5] * a[5] * a[5])};
+        const float dy = S[k] - y;
+        int t = 0;
+#pragma unroll
+        for (int l = 0; l < 5; ++l) {
+#pragma unroll
+            for (int m = 0; m <= l; ++m) A[t++] += d[l] * d[m];
+            B[l] += dy * d[l];
+        }
+        c2 += dy * dy;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int k = 0; k < 15; ++k) A[k] += __shfl_xor_sync(0xffffffffu, A[k], o);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) B[k] += __shfl_xor_sync(0xffffffffu, B[k], o);
+        c2 += __shfl_xor_sync(0xffffffffu, c2, o);
+    }
+    int t = 0;
+#pragma unroll
+    for (int l = 1; l <= 5; ++l) {
+#pragma unroll
+        for (int m = 1; m <= l; ++m) {
+            al[l][m] = A[t];
+            al[m][l] = A[t];
+            ++t;
+        }
+        be[l] = B[l - 1];
+    }
+    chisq = c2;
+}
+
+// Gauss-Jordan with full pivoting (Numerical Recipes gaussj) on the 5 x 5
+// system with one right-hand side; false when singular (the reference would
+// exit; the fit ends instead).
+static __device__ __noinline__ bool gaussj5(float (&m)[6][6], float (&b)[6])
+{
+    int ipiv[6] = {0, 0, 0, 0, 0, 0};
+    int irow = 0, icol = 0;
+    for (int i = 1; i <= 5; i++) {
+        float big = 0.f;
+        for (int j = 1; j <= 5; j++)
+            if (ipiv[j] != 1)
+                for (int k = 1; k <= 5; k++) {
+                    if (ipiv[k] == 0) {
+                        if (fabsf(m[j][k]) >= big) {
+                            big = fabsf(m[j][k]);
+                            irow = j;
+                            icol = k;
+                        }
+                    } else if (ipiv[k] > 1)
+                        return false;
+                }
+        ++ipiv[icol];
+        if (irow != icol) {
+            for (int l = 1; l <= 5; l++) {
+                const float t = m[irow][l];
+                m[irow][l] = m[icol][l];
+                m[icol][l] = t;
+            }
+            const float t = b[irow];
+            b[irow] = b[icol];
+            b[icol] = t;
+        }
+        if (m[icol][icol] == 0.f) return false;
+        const float pivinv = 1.0f / m[icol][icol];
+        m[icol][icol] = 1.f;
+        for (int l = 1; l <= 5; l++) m[icol][l] *= pivinv;
+        b[icol] *= pivinv;
+        for (int ll = 1; ll <= 5; ll++)
+            if (ll != icol) {
+                const float dum = m[ll][icol];
+                m[ll][icol] = 0.f;
+                for (int l = 1; l <= 5; l++) m[ll][l] -= m[icol][l] * dum;
+                b[ll] -= b[icol] * dum;
+            }
+    }
+    return true;
+}
+
+// The fit itself (warp 0); a[1..5] in and out.
+static __device__ __noinline__ void cmp_track_gauss_warp(const float* S, float i0, float j0, float (&a)[6])
+{
+    float alpha[6][6], beta[6], chisq = 0.f, ochisq = 0.f, alamda = -1.f;
+    float lasti = 2e9f, lastj = 2e9f;
+    for (int it = 0; it < 8; ++it) {
+        float covar[6][6], da[6], atry[6];
+        if (alamda < 0.f) {
+            alamda = 0.001f;
+            lm2d_cof(S, i0, j0, a, alpha, beta, chisq);
+            ochisq = chisq;
+        }
+        for (int j = 1; j <= 5; j++) {
+            for (int k = 1; k <= 5; k++) covar[j][k] = alpha[j][k];
+            covar[j][j] = alpha[j][j] * (1.0f + alamda);
+            da[j] = beta[j];
+        }
+        if (!gaussj5(covar, da)) break;
+        atry[0] = a[0];
+        for (int l = 1; l <= 5; l++) atry[l] = a[l] + da[l];
+        lm2d_cof(S, i0, j0, atry, covar, da, chisq);
+        if (chisq < ochisq) {
+            alamda *= 0.1f;
+            ochisq = chisq;
+            for (int j = 1; j <= 5; j++) {
+                for (int k = 1; k <= 5; k++) alpha[j][k] = covar[j][k];
+                beta[j] = da[j];
+            }
+            for (int l = 1; l <= 5; l++) a[l] = atry[l];
+        } else {
+            alamda *= 10.0f;
+            chisq = ochisq;
+        }
+        if (fabsf(a[2] - lasti) < 0.001f && fabsf(a[4] - lastj) < 0.001f) break;
+        lasti = a[2];
+        lastj = a[4];
+    }
+}
+
+// The whole of cmpTrackGauss for one CTA (all threads call it): the edge
+// test on the N x N plane (peaks within 9 of the border, or rejected ones,
+// fail), the 18 x 18 samples mag(i, j) * scale into S, the fit by warp 0
+// (initial amplitude cMax * scale, widths 3), and the result in NOVER units:
+// iMax = round(mux * NOVER), cMax = min(amp, 1); a width above 2000 fails.
+// Failures return iMax = jMax = -LARGEINT and cMax = 0.  g6: 6 floats of
+// shared scratch.
+template <int NT, class Mag>
+__device__ __forceinline__ void gauss2d_peak(Mag mag, int N, double scale, float* S, float* g6, int& iMax, int& jMax,
+                                             double& cMax)
+{
+    if ((iMax - NGAUSS / 2) < 0 || (iMax + NGAUSS / 2) >= (N - 1) || (jMax - NGAUSS / 2) < 0 ||
+        (jMax + NGAUSS / 2) >= (N - 1)) {
+        iMax = -(int)SB_LARGEINT;
+        jMax = -(int)SB_LARGEINT;
+        cMax = 0.0;
+        return;
+    }
+    const int tid = threadIdx.x;
+    for (int e = tid; e < NGAUSS * NGAUSS; e += NT)
+        S[e] = (float)((double)mag(iMax - NGAUSS / 2 + e / NGAUSS, jMax - NGAUSS / 2 + e % NGAUSS) * scale);
+    __syncthreads();
+    if (tid < 32) {
+        float g[6] = {0.f, (float)(cMax * scale), (float)iMax, 3.f, (float)jMax, 3.f};
+        cmp_track_gauss_warp(S, (float)(iMax - NGAUSS / 2), (float)(jMax - NGAUSS / 2), g);
+        if (tid < 6) g6[tid] = g[tid];
+    }
+    __syncthreads();
+    const float g1 = g6[1], g2 = g6[2], g3 = g6[3], g4 = g6[4], g5 = g6[5];
+    __syncthreads();
+    iMax = (int)round((double)(g2 * NOVER));
+    jMax = (int)round((double)(g4 * NOVER));
+    cMax = g1 < 1.0f ? (double)g1 : 1.0;
+    if ((0.5 * g3) > 1000.0 || (0.5 * g5) > 1000.0) {
+        iMax = -(int)SB_LARGEINT;
+        jMax = -(int)SB_LARGEINT;
+        cMax = 0.0;
+    }
 }
 
 }  // namespace sbk

@@ -37,6 +37,7 @@ struct CmplxArgs {
     int intNr, intNa, intNrl, intNal, intMSB;
     int intPs, intPSA, intPSR;  // patch, padded sizes (ps * nal, ps * nrl)
     const float2* twP;          // exp(-2 pi i e / ps), e < ps
+    int gauss;                  // -gauss: 2-D Gaussian fit instead of the oversampling
 };
 
 // Arguments of an amplitude try (small: s = 1, large: s = LA = 2).
@@ -66,6 +67,7 @@ struct AmpArgs {
     size_t scratchPerCta; // float2 elements
     PointRec* rec;
     FitJob* fit;
+    int gauss;            // -gauss: 2-D Gaussian fit instead of the oversampling
 };
 
 bool cmplx_supported(int W);

@@ -254,3 +254,22 @@ def test_interferogram_flattening_restores_matches():
     # looks that make the padded patch smaller than the window are refused
     with pytest.raises(RuntimeError):
         oracle.strack(abi.TrackParams(**base, intf=dict(data=intf, nrl=3, nal=3)), a, b)
+
+
+@pytest.mark.parametrize("dr,da", [(3, -2), (1.25, -0.5), (-2.4, 0.3)])
+def test_gauss_fit_recovers_shift(dr, da):
+    """-gauss (cmpTrackGauss): the 18 x 18 Gaussian fit places band-limited
+    shifts within the 1/24 px quantum in the complex stage and within 1/8 px
+    in the amplitude stage; the float oracle gives the same offsets."""
+    z = _speckle(256, 256, 12)
+    z2 = _fourier_shift(z, da, dr)
+    for nc, tol in ((0, 1 / 24), (1, 1 / 8)):
+        p = _params(gaussFlag=1, noComplex=nc)
+        o = oracle.strack(p, z.astype(np.complex64), z2.astype(np.complex64))
+        assert (o["type"] == (abi.SB_AMPMATCH if nc else abi.SB_CMATCH)).all()
+        assert np.abs(o["offR"] - dr).max() <= tol + 1e-6
+        assert np.abs(o["offA"] - da).max() <= tol + 1e-6
+        assert (o["corr"] <= 1.0).all() and (o["corr"] > 0.185).all()
+        f = oracle.strack(p, z.astype(np.complex64), z2.astype(np.complex64), precision="f32")
+        assert np.array_equal(f["offR"], o["offR"]) and np.array_equal(f["offA"], o["offA"])
+

@@ -188,3 +188,36 @@ def test_interferogram_phase_correction(ctx):
     with pytest.raises(Exception, match="smaller than the window"):
         ctx.strack(abi.TrackParams(rStart=48, aStart=48, deltaR=16, deltaA=16, nR=4, nA=4,
                                    intf=dict(data=intf, nrl=3, nal=3)), a, b)
+
+
+@pytest.mark.parametrize("kw", [
+    dict(),                                                      # complex matches, 2-D fit on the 2x grid
+    dict(noComplex=1),                                           # amplitude: shared-memory kernel (Ws 32)
+    dict(noComplex=1, wRa=48, wAa=48, rStart=56, aStart=56),     # amplitude: staged kernel (Ws 48)
+    dict(wR=64, wA=64, wRa=64, wAa=64, deltaR=24, deltaA=24, nR=36, nA=16, rStart=64, aStart=64),
+])
+def test_gauss_fit_mode(ctx, pair_1k, kw):
+    """-gauss (cmpTrackGauss, speckleTrack.c:2205-2303): the 18 x 18 Gaussian
+    fit replaces the 8x8 -> 96x96 oversampling in the complex and amplitude
+    stages; offsets and match types against the oracle at the usual bar."""
+    a, b = pair_1k
+    p = _p(gaussFlag=1, **kw)
+    g, o, st = _check(ctx, p, a, b)
+    assert st["n_match_oracle"] > 300
+    d = ctx.strack(_p(**kw), a, b)
+    ok = (g["type"] > 0) & (d["type"] > 0)
+    moved = (g["offR"][ok] != d["offR"][ok]) | (g["offA"][ok] != d["offA"][ok])
+    assert moved.mean() > 0.2  # the fit, not the oversampling, placed the peaks
+
+
+def test_gauss_fit_moderate_coherence(ctx):
+    """-gauss at coherence 0.55: complex fits fail for about half the points
+    and both amplitude tries (32 and 64 windows) place the rest.  (The
+    Gaussian has no background term, so at coherence 0.25 the fit settles on
+    broad, weak peaks and every point fails, in the oracle as on the GPU.)"""
+    s1, s2 = synth.make_pair(512, 512, 21, dr=lambda y, x: 1.3 + 0 * x, da=lambda y, x: -0.6 + 0 * y,
+                             coherence=0.55)
+    a, b = synth.to_numpy(s1), synth.to_numpy(s2)
+    p = _p(rStart=72, aStart=72, nR=24, nA=24, deltaR=16, deltaA=16, gaussFlag=1)
+    g, o, st = _check(ctx, p, a, b)
+    assert o["stats"]["nAmp"] > 20 and o["stats"]["nAmpL"] > 100 and o["stats"]["nComplex"] > 100
