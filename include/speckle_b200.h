@@ -268,6 +268,50 @@ int sb_cull_smooth(sb_context *ctx, const sb_cull_params *p, sb_cull_data *d);
 int sb_cull_islands(sb_context *ctx, const sb_cull_params *p, sb_cull_data *d);
 
 /* ------------------------------------------------------------------------ */
+/* Culling Landsat offsets (cullls)                                          */
+/* ------------------------------------------------------------------------ */
+
+/* CullLSParams (Cullls/cullls.h:2-35) restricted to the values the passes
+ * read, plus the values cullls takes from landsatSource64 headers that are
+ * not part of the reference tree (lstrack.h, lsfit.h, common.h): the caller
+ * supplies them.  X is the column (range-like) offset, Y the row offset. */
+typedef struct {
+    int32_t nx, ny;        /* matches.nx, matches.ny: grid columns and rows */
+    int32_t boxSize;       /* -boxSize (bR = bA; cullls default 9) */
+    int32_t nGood;         /* -nGood (default 17) */
+    float maxX, maxY;      /* -maxX (.75) -maxY (1.0): median deviation limits */
+    int32_t sX, sY;        /* -sx -sy (3): smoothing box */
+    int32_t islandThresh;  /* -islandThresh (<=0: no island pass; default -1) */
+    int32_t nCullPasses;   /* cullLSData repetitions; cullls runs 3 */
+    int32_t connectivity;  /* island labelling: 8 (default) or 4 */
+    double deltaT;         /* fitDat.deltaT, days between the images */
+    double dx, dy;         /* matches.dx, matches.dy: pixel size (m) */
+    double noDataLimit;    /* NODATA + 1 as the Y > NODATA + 1 test sees it */
+    double nOver;          /* lstrack's NOVER (quantisation 1/nOver px), > 0 */
+    uint8_t slowVelMask;   /* SLOWVEL bit(s) of matches.type */
+    uint8_t noDataMask;    /* NODATATOUSE bit(s) of matches.type */
+    uint8_t reserved[6];
+} sb_cullls_params;
+
+/* Buffers of one cullls job (host memory unless onDevice). */
+typedef struct {
+    float *X, *Y;          /* in/out: cullLSData culls them in place */
+    const uint8_t *type;   /* in: matches.type */
+    float *XS, *YS;        /* out: smoothed offsets (.cull.dx/.cull.dy) */
+    float *sigmaX, *sigmaY; /* out: sigmas (.cull.sx/.cull.sy) */
+    int32_t onDevice;
+    int64_t nAttempt;      /* out: points with (type & noDataMask) == 0, before culling */
+    int64_t nMatch;        /* out: valid points before culling */
+    int64_t nCulled;       /* out: points culled by the last cullLSData pass */
+    int64_t nIslands, nIslandPoints; /* out */
+} sb_cullls_data;
+
+/* Whole cullls pipeline of Cullls/cullls.c:23-56: cullLSData x nCullPasses,
+ * cullLSStats, cullLSSmooth, cullLSIslands (cullLSData.c:13-138,
+ * cullLSStats.c:19-157, cullLSSmooth.c:11-73, cullLSIslands.c:15-174). */
+int sb_cullls(sb_context *ctx, const sb_cullls_params *p, sb_cullls_data *d);
+
+/* ------------------------------------------------------------------------ */
 /* Allocation-free amplitude correlation                                     */
 /* ------------------------------------------------------------------------ */
 

@@ -15,6 +15,10 @@
  *    scan; 8-connectivity unless connectivity == 4.  This is an assumption
  *    (the routine's source is not available); island culling is pinned to
  *    this labelling.
+ * cullls (Cullls/cullls.c:23-56, cullLSData.c, cullLSStats.c, cullLSSmooth.c,
+ * cullLSIslands.c) shares the stats and islands passes; the landsatSource64
+ * values it reads (SLOWVEL, NODATATOUSE, NODATA, NOVER, the lsFit/matchResult
+ * fields) come from headers absent from the tree and are inputs here.
  * LARGEINT is 2e9 (clib) except in cullst.c, which redefines it as -2e9, so
  * addSubtractSimOffsets applies to every finite point (cullst.c:11,115).
  */
@@ -191,15 +195,17 @@ static void planeFit(const double *x0, const float *xs, const float *ys, const d
     }
 }
 
-int oracle_cull_stats(const sb_cull_params *p, sb_cull_data *d)
+/* cullStats.c:19-144 (box fixed at 9x9, :38-39); cullLSStats.c:19-157 is
+ * the same with qvar = (1/NOVER)^2/12 added to the variances before the root
+ * (:147-148). */
+static void stats_core(int nR, int nA, const float *offR, const float *offA, float *sigmaR, float *sigmaA,
+                       double qvar)
 {
-    /* cullStats.c:19-144 (box fixed at 9x9, :38-39) */
-    const int nR = p->nR, nA = p->nA, bR = 9, bA = 9;
+    const int bR = 9, bA = 9;
     const int cap = 1 + (bR + 1) * (bA + 1);
     double *listR = (double *)malloc(sizeof(double) * cap), *listA = (double *)malloc(sizeof(double) * cap);
     float *xs = (float *)malloc(sizeof(float) * cap), *ys = (float *)malloc(sizeof(float) * cap);
     double aR[4] = {0, 0, 0, 0}, aA[4] = {0, 0, 0, 0};
-    const float *offR = d->offR, *offA = d->offA;
     for (int i = 0; i < nA; i++) {
         int i1 = i - bA / 2 > 0 ? i - bA / 2 : 0;
         int i2 = i + bA / 2 < nA - 1 ? i + bA / 2 : nA - 1;
@@ -259,15 +265,24 @@ int oracle_cull_stats(const sb_cull_params *p, sb_cull_data *d)
                 sR = (float)(sR - meanR * meanR / (float)((ngood - 3) * ngood));
                 sA = (float)(0.00001 > sA ? 0.00001 : sA);
                 sR = (float)(0.00001 > sR ? 0.00001 : sR);
-                d->sigmaA[k] = (float)sqrt((double)sA);
-                d->sigmaR[k] = (float)sqrt((double)sR);
+                if (qvar != 0.0) {
+                    sR += qvar;
+                    sA += qvar;
+                }
+                sigmaA[k] = (float)sqrt((double)sA);
+                sigmaR[k] = (float)sqrt((double)sR);
             } else {
-                d->sigmaA[k] = (float)-LARGEINT;
-                d->sigmaR[k] = (float)-LARGEINT;
+                sigmaA[k] = (float)-LARGEINT;
+                sigmaR[k] = (float)-LARGEINT;
             }
         }
     }
     free(listR); free(listA); free(xs); free(ys);
+}
+
+int oracle_cull_stats(const sb_cull_params *p, sb_cull_data *d)
+{
+    stats_core(p->nR, p->nA, d->offR, d->offA, d->sigmaR, d->sigmaA, 0.0);
     return SB_OK;
 }
 
@@ -341,15 +356,16 @@ static int32_t uf_find(int32_t *par, int32_t x)
     return x;
 }
 
-int oracle_cull_islands(const sb_cull_params *p, sb_cull_data *d)
+/* cullIslands.c:13-168 + screenIslands :173-198 (cullLSIslands.c:15-204 is
+ * the same on XS/YS) */
+static void islands_core(int nR, int nA, int connectivity, int islandThresh, float *offRS, float *offAS,
+                         int64_t *nIslands, int64_t *nIslandPoints)
 {
-    /* cullIslands.c:13-168 + screenIslands :173-198 */
-    const int nR = p->nR, nA = p->nA;
     const size_t n = (size_t)nR * nA;
     const float regionMin = (float)(-LARGEINT + 1000);
     int32_t *par = (int32_t *)malloc(sizeof(int32_t) * n);
-    for (size_t k = 0; k < n; k++) par[k] = d->offRS[k] >= regionMin ? (int32_t)k : -1;
-    const int conn8 = (p->connectivity != 4);
+    for (size_t k = 0; k < n; k++) par[k] = offRS[k] >= regionMin ? (int32_t)k : -1;
+    const int conn8 = (connectivity != 4);
     for (int i = 0; i < nA; i++)
         for (int j = 0; j < nR; j++) {
             size_t k = (size_t)i * nR + j;
@@ -393,19 +409,25 @@ int oracle_cull_islands(const sb_cull_params *p, sb_cull_data *d)
     int64_t nIsl = 0, nPts = 0;
     char *cull = (char *)calloc((size_t)K + 1, 1);
     for (int32_t l = 1; l < K; l++) { /* label K is skipped, as in the reference */
-        if ((maxX[l] - minX[l]) > p->islandThresh || (maxY[l] - minY[l]) > p->islandThresh) continue;
+        if ((maxX[l] - minX[l]) > islandThresh || (maxY[l] - minY[l]) > islandThresh) continue;
         cull[l] = 1;
         nIsl++;
     }
     for (size_t k = 0; k < n; k++)
         if (label[k] > 0 && cull[label[k]]) {
-            d->offRS[k] = (float)-LARGEINT;
-            if (d->offAS) d->offAS[k] = (float)-LARGEINT;
+            offRS[k] = (float)-LARGEINT;
+            if (offAS) offAS[k] = (float)-LARGEINT;
             nPts++;
         }
-    d->nIslands = nIsl;
-    d->nIslandPoints = nPts;
+    *nIslands = nIsl;
+    *nIslandPoints = nPts;
     free(par); free(label); free(minX); free(maxX); free(minY); free(maxY); free(cull);
+}
+
+int oracle_cull_islands(const sb_cull_params *p, sb_cull_data *d)
+{
+    islands_core(p->nR, p->nA, p->connectivity, p->islandThresh, d->offRS, d->offAS, &d->nIslands,
+                 &d->nIslandPoints);
     return SB_OK;
 }
 
@@ -419,5 +441,134 @@ int oracle_cull(const sb_cull_params *p, sb_cull_data *d)
     if (p->useSim) addSubtractSim(p, d, 1.0f);
     oracle_cull_smooth(p, d);
     if (p->islandThresh > 0) oracle_cull_islands(p, d);
+    return SB_OK;
+}
+
+/* ---------------------------------------------------------------- cullls */
+
+/* cullLSData.c:13-138: the cullSTData median test on X (columns) and Y
+ * (rows) without the corr/mask pre-pass.  A point is kept when more than
+ * nGood box points are valid, Y > NODATA + 1, and both deviations from the
+ * box medians are within the limits; the limits are 40 m/yr * deltaT / pixel
+ * size (at least 0.2) when every valid box point carries the SLOWVEL bit,
+ * else maxX/maxY.  The first pass also counts the valid points (nMatch) and
+ * the points with data (nAttempt). */
+static void cullls_data(const sb_cullls_params *p, sb_cullls_data *d, int first)
+{
+    const int nx = p->nx, ny = p->ny;
+    float *X = d->X, *Y = d->Y;
+    const int bR = p->boxSize, bA = p->boxSize;
+    float *listX = (float *)malloc(sizeof(float) * (size_t)(1000 + (bR + 1) * (bA + 1)));
+    float *listY = (float *)malloc(sizeof(float) * (size_t)(1000 + (bR + 1) * (bA + 1)));
+    if (first) {
+        int64_t nGoodPts = 0, nWithData = 0;
+        for (size_t k = 0; k < (size_t)nx * ny; k++) {
+            if (validPt(X[k], Y[k])) nGoodPts++;
+            if ((d->type[k] & p->noDataMask) == 0) nWithData++;
+        }
+        d->nAttempt = nWithData;
+        d->nMatch = nGoodPts;
+    }
+    double slowX = 40.0 / 365. * p->deltaT, slowY = slowX;
+    slowX /= p->dx;
+    slowY /= p->dy;
+    slowX = slowX > 0.2 ? slowX : 0.2;
+    slowY = slowY > 0.2 ? slowY : 0.2;
+    int64_t nCulled = 0;
+    for (int i = 0; i < ny; i++) {
+        int i1 = i - bA / 2 > 0 ? i - bA / 2 : 0;
+        int i2 = i + bA / 2 < ny - 1 ? i + bA / 2 : ny - 1;
+        for (int j = 0; j < nx; j++) {
+            int j1 = j - bR / 2 > 0 ? j - bR / 2 : 0;
+            int j2 = j + bR / 2 < nx - 1 ? j + bR / 2 : nx - 1;
+            int slowFlag = TRUE;
+            uint32_t ngood = 0;
+            for (int ii = i1; ii <= i2; ii++)
+                for (int jj = j1; jj <= j2; jj++) {
+                    size_t kk = (size_t)ii * nx + jj;
+                    if (validPt(X[kk], Y[kk])) {
+                        listX[ngood] = X[kk];
+                        listY[ngood] = Y[kk];
+                        ngood++;
+                        if (!(d->type[kk] & p->slowVelMask)) slowFlag = FALSE;
+                    }
+                }
+            size_t k = (size_t)i * nx + j;
+            if (ngood > (uint32_t)p->nGood && (double)Y[k] > p->noDataLimit) {
+                uint32_t midIndex = ngood / 2;
+                if (midIndex < 1) midIndex = 1;
+                qsort(listX, ngood, sizeof(float), cmpf);
+                qsort(listY, ngood, sizeof(float), cmpf);
+                float medianX = listX[midIndex - 1], medianY = listY[midIndex - 1];
+                double diffY = (double)(Y[k] - medianY);
+                double diffX = (double)(X[k] - medianX);
+                double maxX = slowFlag ? slowX : (double)p->maxX;
+                double maxY = slowFlag ? slowY : (double)p->maxY;
+                if (fabs(diffY) > maxY || fabs(diffX) > maxX) {
+                    X[k] = (float)-LARGEINT;
+                    Y[k] = (float)-LARGEINT;
+                    nCulled++;
+                }
+            } else {
+                X[k] = (float)-LARGEINT;
+                Y[k] = (float)-LARGEINT;
+                nCulled++;
+            }
+        }
+    }
+    d->nCulled = nCulled;
+    free(listX);
+    free(listY);
+}
+
+/* cullLSSmooth.c:29-70: unweighted box mean, one look per valid point. */
+static void cullls_smooth(const sb_cullls_params *p, sb_cullls_data *d)
+{
+    const int nx = p->nx, ny = p->ny;
+    for (int i = 0; i < ny; i++) {
+        int i1 = i - p->sY / 2 > 0 ? i - p->sY / 2 : 0;
+        int i2 = i + p->sY / 2 < ny - 1 ? i + p->sY / 2 : ny - 1;
+        for (int j = 0; j < nx; j++) {
+            int j1 = j - p->sX / 2 > 0 ? j - p->sX / 2 : 0;
+            int j2 = j + p->sX / 2 < nx - 1 ? j + p->sX / 2 : nx - 1;
+            uint32_t ngood = 0;
+            float nLooksEff = 0.0f;
+            double meanY = 0.0, meanX = 0.0;
+            for (int ii = i1; ii <= i2; ii++)
+                for (int jj = j1; jj <= j2; jj++) {
+                    size_t kk = (size_t)ii * nx + jj;
+                    if (validPt(d->X[kk], d->Y[kk])) {
+                        ngood++;
+                        nLooksEff++;
+                        meanY += d->Y[kk];
+                        meanX += d->X[kk];
+                    }
+                }
+            size_t k = (size_t)i * nx + j;
+            if (((ngood > 1) || (p->sY == 1) || (p->sX == 1)) && d->X[k] > (float)(1 - LARGEINT) &&
+                d->sigmaY[k] > (float)(1 - LARGEINT)) {
+                nLooksEff = (float)((double)nLooksEff > 1. ? (double)nLooksEff : 1.);
+                d->sigmaY[k] = (float)(d->sigmaY[k] / sqrt((double)nLooksEff));
+                d->sigmaX[k] = (float)(d->sigmaX[k] / sqrt((double)nLooksEff));
+                d->XS[k] = (float)(meanX / (float)ngood);
+                d->YS[k] = (float)(meanY / (float)ngood);
+            } else {
+                d->XS[k] = (float)-LARGEINT;
+                d->YS[k] = (float)-LARGEINT;
+            }
+        }
+    }
+}
+
+int oracle_cullls(const sb_cullls_params *p, sb_cullls_data *d)
+{
+    /* cullls.c:23-56 */
+    int passes = p->nCullPasses > 0 ? p->nCullPasses : 3;
+    for (int k = 0; k < passes; k++) cullls_data(p, d, k == 0);
+    stats_core(p->nx, p->ny, d->X, d->Y, d->sigmaX, d->sigmaY, ((1.0 / p->nOver) * (1.0 / p->nOver)) / 12.);
+    cullls_smooth(p, d);
+    d->nIslands = d->nIslandPoints = 0;
+    if (p->islandThresh > 0)
+        islands_core(p->nx, p->ny, p->connectivity, p->islandThresh, d->XS, d->YS, &d->nIslands, &d->nIslandPoints);
     return SB_OK;
 }

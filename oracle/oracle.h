@@ -40,6 +40,9 @@ int oracle_cull_stats(const sb_cull_params *p, sb_cull_data *d);
 int oracle_cull_smooth(const sb_cull_params *p, sb_cull_data *d);
 int oracle_cull_islands(const sb_cull_params *p, sb_cull_data *d);
 
+/* cullls pipeline (Cullls/cullls.c:23-56). */
+int oracle_cullls(const sb_cullls_params *p, sb_cullls_data *d);
+
 /* estDopCarrier1 (Strack/dopplerEstimation.c:25-40) on one pair of
  * interleaved complex patches (float32 re,im), returning the roll scaled to wA. */
 int oracle_est_dop_carrier(const float *p1, const float *p2, int32_t nAz, int32_t nRg,

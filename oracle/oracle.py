@@ -37,6 +37,8 @@ def lib(precision="f64"):
             f = getattr(L, name)
             f.argtypes = [C.POINTER(abi.SbCullParams), C.POINTER(abi.SbCullData)]
             f.restype = C.c_int
+        L.oracle_cullls.argtypes = [C.POINTER(abi.SbCulllsParams), C.POINTER(abi.SbCulllsData)]
+        L.oracle_cullls.restype = C.c_int
         L.oracle_est_dop_carrier.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32]
         L.oracle_est_dop_carrier.restype = C.c_int
         L.oracle_fft2d.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]
@@ -104,6 +106,18 @@ def cull(params, offR, offA, corr, mtype, mask=None, simR=None, simA=None, passe
     d["nCulled"] = cd.nCulled
     d["nIslands"] = cd.nIslands
     d["nIslandPoints"] = cd.nIslandPoints
+    return d
+
+
+def cullls(params, X, Y, mtype):
+    """cullls pipeline (Cullls/cullls.c:23-56)."""
+    d, cd = abi.cullls_data(X, Y, mtype)
+    p = params.to_c()
+    rc = lib("f64").oracle_cullls(C.byref(p), C.byref(cd))
+    if rc != abi.SB_OK:
+        raise RuntimeError(f"oracle cullls returned {rc}")
+    for k in ("nAttempt", "nMatch", "nCulled", "nIslands", "nIslandPoints"):
+        d[k] = getattr(cd, k)
     return d
 
 

@@ -155,6 +155,41 @@ class SbCullData(C.Structure):
     ]
 
 
+class SbCulllsParams(C.Structure):
+    _fields_ = [
+        ("nx", _i32), ("ny", _i32),
+        ("boxSize", _i32),
+        ("nGood", _i32),
+        ("maxX", _f32), ("maxY", _f32),
+        ("sX", _i32), ("sY", _i32),
+        ("islandThresh", _i32),
+        ("nCullPasses", _i32),
+        ("connectivity", _i32),
+        ("deltaT", C.c_double),
+        ("dx", C.c_double), ("dy", C.c_double),
+        ("noDataLimit", C.c_double),
+        ("nOver", C.c_double),
+        ("slowVelMask", C.c_uint8),
+        ("noDataMask", C.c_uint8),
+        ("reserved", C.c_uint8 * 6),
+    ]
+
+
+class SbCulllsData(C.Structure):
+    _fields_ = [
+        ("X", C.c_void_p), ("Y", C.c_void_p),
+        ("type", C.c_void_p),
+        ("XS", C.c_void_p), ("YS", C.c_void_p),
+        ("sigmaX", C.c_void_p), ("sigmaY", C.c_void_p),
+        ("onDevice", _i32),
+        ("nAttempt", _i64),
+        ("nMatch", _i64),
+        ("nCulled", _i64),
+        ("nIslands", _i64),
+        ("nIslandPoints", _i64),
+    ]
+
+
 def ptr(a):
     """Address of a numpy array (or None)."""
     if a is None:
@@ -280,6 +315,63 @@ class CullParams:
         p = SbCullParams()
         for name, _ in SbCullParams._fields_:
             setattr(p, name, getattr(self, name))
+        return p
+
+
+def cullls_data(X, Y, mtype):
+    """Host buffers of one cullls job: copies of X, Y, type and zeroed
+    outputs; returns (dict of arrays, SbCulllsData over them)."""
+    ny, nx = X.shape
+    d = {
+        "X": np.array(X, np.float32, copy=True),
+        "Y": np.array(Y, np.float32, copy=True),
+        "type": np.array(mtype, np.uint8, copy=True),
+        "XS": np.zeros((ny, nx), np.float32),
+        "YS": np.zeros((ny, nx), np.float32),
+        "sigmaX": np.zeros((ny, nx), np.float32),
+        "sigmaY": np.zeros((ny, nx), np.float32),
+    }
+    cd = SbCulllsData(*[ptr(d[k]) for k in ("X", "Y", "type", "XS", "YS", "sigmaX", "sigmaY")], 0, 0, 0, 0, 0, 0)
+    return d, cd
+
+
+class CullLSParams:
+    """Mirror of the reference's CullLSParams (Cullls/cullls.h:2-35) with the
+    cullls CLI defaults (Cullls/cullls.c:184-191), plus the landsatSource64
+    values cullls reads from headers that are not in the reference tree:
+    deltaT (days), dx/dy (pixel size, m), slowVelMask (SLOWVEL), noDataMask
+    (NODATATOUSE), noDataLimit (NODATA + 1) and nOver (lstrack's NOVER, no
+    default: it must be given)."""
+
+    def __init__(self, **kw):
+        self.nx = 0
+        self.ny = 0
+        self.boxSize = 9
+        self.nGood = 17
+        self.maxX = 0.75
+        self.maxY = 1.0
+        self.sX = 3
+        self.sY = 3
+        self.islandThresh = -1
+        self.nCullPasses = 3
+        self.connectivity = 8
+        self.deltaT = 0.0
+        self.dx = 0.0
+        self.dy = 0.0
+        self.noDataLimit = -1999999999.0
+        self.nOver = 0.0
+        self.slowVelMask = 0
+        self.noDataMask = 0
+        for k, v in kw.items():
+            if not hasattr(self, k):
+                raise TypeError(f"unknown cullls parameter {k!r}")
+            setattr(self, k, v)
+
+    def to_c(self):
+        p = SbCulllsParams()
+        for name, _ in SbCulllsParams._fields_:
+            if name != "reserved":
+                setattr(p, name, getattr(self, name))
         return p
 
 

@@ -17,6 +17,11 @@
 //    thread per point.  The plane fit is least squares with singular values
 //    below 1e-5 * max dropped (svdfit), via the 3x3 normal matrix's Jacobi
 //    eigen-decomposition, in double precision.
+//  cullls (Cullls/cullls.c:23-56) runs the same kernels: its median pass
+//    (cullLSData.c:13-138) adds the slow-flow limits and the NODATA test to
+//    the decision rule (StRule), its stats (cullLSStats.c) the quantisation
+//    variance, its smoothing (cullLSSmooth.c) is the unweighted box mean of
+//    cullls_smooth_kernel, and its islands pass is cullIslands'.
 //  cullIslands (cullIslands.c:13-198): union-find labelling (links to the
 //    smaller index, so each root is its component's first pixel in raster
 //    order), labels numbered by first appearance, bounding boxes, and the cull
@@ -37,6 +42,21 @@ __device__ __forceinline__ bool valid_pt(float r, float a) { return r > kValidLi
 
 // ---------------------------------------------------------------- pre-pass
 
+// The decision rule of one median pass.  cullst (cullSTData.c:80-123): cull
+// unless more than nGood valid neighbours and both deviations from the box
+// medians within maxA/maxR.  cullls (cullLSData.c:63-134) adds: the limits
+// become slowMaxA/slowMaxR when every valid point of the box carries a
+// slowMask bit in slowType, and the point's own offA must exceed selfLim.
+struct StRule {
+    int nGood;
+    double maxR, maxA;
+    double slowMaxR, slowMaxA;
+    const uint8_t* slowType;  // null: no slow-flow test (cullst)
+    unsigned slowMask;
+    bool selfTest;            // cullls: the point's offA must exceed selfLim (false for NaN)
+    double selfLim;
+};
+
 struct CullArgs {
     float* offR;
     float* offA;
@@ -44,8 +64,9 @@ struct CullArgs {
     uint8_t* type;
     const uint8_t* mask;
     int nR, nA;
-    int bR, bA, nGood;
-    float maxA, maxR, corrThresh;
+    int bR, bA;
+    StRule rule;
+    float corrThresh;
     int singleMT;
     int* rowCounter;
     int* progress;
@@ -110,6 +131,25 @@ __device__ __forceinline__ uint32_t warp_kth(const uint32_t (&key)[NV], uint32_t
     return prefix;
 }
 
+// One point's decision, by a whole warp (uniform result).  kr/ka: the lanes'
+// keys of the valid box points (vm), notSlow: this lane saw a valid point
+// without the slow bit; oR/oA: the point's own offsets.
+template <int NV>
+__device__ __forceinline__ bool st_decide(const StRule& r, const uint32_t (&kr)[NV], const uint32_t (&ka)[NV],
+                                          uint32_t vm, int ngood, bool notSlow, float oR, float oA)
+{
+    const bool slow = r.slowType != nullptr && !__any_sync(0xffffffffu, notSlow);
+    if ((unsigned)ngood > (unsigned)r.nGood && (!r.selfTest || (double)oA > r.selfLim)) {
+        int mid = ngood / 2;
+        if (mid < 1) mid = 1;
+        const float medR = fkey_inv(warp_kth<NV>(kr, vm, mid));
+        const float medA = fkey_inv(warp_kth<NV>(ka, vm, mid));
+        const double dA = (double)(oA - medA), dR = (double)(oR - medR);
+        return fabs(dA) > (slow ? r.slowMaxA : r.maxA) || fabs(dR) > (slow ? r.slowMaxR : r.maxR);
+    }
+    return true;
+}
+
 template <int NV>
 __global__ void cull_median_kernel(CullArgs a, long long spinLimit)
 {
@@ -156,6 +196,7 @@ __global__ void cull_median_kernel(CullArgs a, long long spinLimit)
             const int cnt = rows * cols;
             uint32_t kr[NV], ka[NV];
             uint32_t vm = 0;
+            bool notSlow = false;
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
                 const int e = lane + 32 * v;
@@ -168,6 +209,7 @@ __global__ void cull_median_kernel(CullArgs a, long long spinLimit)
                         vm |= 1u << v;
                         kr[v] = fkey(r);
                         ka[v] = fkey(az);
+                        if (a.rule.slowType && !(a.rule.slowType[q] & a.rule.slowMask)) notSlow = true;
                     }
                 }
             }
@@ -176,18 +218,8 @@ __global__ void cull_median_kernel(CullArgs a, long long spinLimit)
             for (int v = 0; v < NV; ++v) ngood += (vm >> v) & 1u;
             ngood = __reduce_add_sync(0xffffffffu, ngood);
             const size_t c = (size_t)row * a.nR + j;
-            bool cull;
-            if ((unsigned)ngood > (unsigned)a.nGood) {
-                int mid = ngood / 2;
-                if (mid < 1) mid = 1;
-                const float medR = fkey_inv(warp_kth<NV>(kr, vm, mid));
-                const float medA = fkey_inv(warp_kth<NV>(ka, vm, mid));
-                const float oR = __ldcg(&a.offR[c]), oA = __ldcg(&a.offA[c]);
-                const double dA = (double)(oA - medA), dR = (double)(oR - medR);
-                cull = fabs(dA) > a.maxA || fabs(dR) > a.maxR;
-            } else {
-                cull = true;
-            }
+            const bool cull =
+                st_decide<NV>(a.rule, kr, ka, vm, ngood, notSlow, __ldcg(&a.offR[c]), __ldcg(&a.offA[c]));
             if (lane == 0) {
                 if (cull) {
                     a.offR[c] = kCulled;
@@ -228,8 +260,8 @@ struct FixArgs {
     uint8_t* cout;
     const uint8_t* chgIn;  // null: first step, every point computed
     uint8_t* chgOut;
-    int nR, nA, bR, bA, nGood;
-    float maxA, maxR;
+    int nR, nA, bR, bA;
+    StRule rule;
     unsigned int* nChanged;
 };
 
@@ -263,6 +295,7 @@ __global__ void cull_fix_kernel(FixArgs a)
         }
         uint32_t kr[NV], ka[NV];
         uint32_t vm = 0;
+        bool notSlow = false;
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
             const int e = lane + 32 * v;
@@ -274,6 +307,7 @@ __global__ void cull_fix_kernel(FixArgs a)
                     vm |= 1u << v;
                     kr[v] = fkey(r);
                     ka[v] = fkey(az);
+                    if (a.rule.slowType && !(a.rule.slowType[q] & a.rule.slowMask)) notSlow = true;
                 }
             }
         }
@@ -281,18 +315,7 @@ __global__ void cull_fix_kernel(FixArgs a)
 #pragma unroll
         for (int v = 0; v < NV; ++v) ngood += (vm >> v) & 1u;
         ngood = __reduce_add_sync(0xffffffffu, ngood);
-        bool cull;
-        if ((unsigned)ngood > (unsigned)a.nGood) {
-            int mid = ngood / 2;
-            if (mid < 1) mid = 1;
-            const float medR = fkey_inv(warp_kth<NV>(kr, vm, mid));
-            const float medA = fkey_inv(warp_kth<NV>(ka, vm, mid));
-            const float oR = a.offR[p], oA = a.offA[p];
-            const double dA = (double)(oA - medA), dR = (double)(oR - medR);
-            cull = fabs(dA) > a.maxA || fabs(dR) > a.maxR;
-        } else {
-            cull = true;
-        }
+        const bool cull = st_decide<NV>(a.rule, kr, ka, vm, ngood, notSlow, a.offR[p], a.offA[p]);
         if (lane == 0) {
             const uint8_t c = cull ? 1 : 0;
             a.cout[p] = c;
@@ -395,6 +418,7 @@ struct StatsArgs {
     float* sigmaR;
     float* sigmaA;
     int nR, nA;
+    double qvar;  // cullls: quantisation variance (1/NOVER)^2/12 added before the root; 0 for cullst
 };
 
 __global__ void cull_stats_kernel(StatsArgs a)
@@ -454,6 +478,10 @@ __global__ void cull_stats_kernel(StatsArgs a)
         sR = (float)((double)sR - meanR * meanR / (float)((ngood - 3) * ngood));
         sA = (float)(0.00001 > (double)sA ? 0.00001 : (double)sA);
         sR = (float)(0.00001 > (double)sR ? 0.00001 : (double)sR);
+        if (a.qvar != 0.0) {  // cullLSStats.c:147-148
+            sR = (float)((double)sR + a.qvar);
+            sA = (float)((double)sA + a.qvar);
+        }
         a.sigmaA[k] = (float)sqrt((double)sA);
         a.sigmaR[k] = (float)sqrt((double)sR);
     } else {
@@ -513,6 +541,58 @@ __global__ void cull_smooth_kernel(SmoothArgs a)
     } else {
         a.offRS[k] = kCulled;
         a.offAS[k] = kCulled;
+    }
+}
+
+// cullLSSmooth.c:29-70: the unweighted mean over the sA x sR box, one look
+// per valid point.
+__global__ void cullls_smooth_kernel(SmoothArgs a)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.nR * a.nA) return;
+    const int i = k / a.nR, j = k % a.nR;
+    const int i1 = i - a.sA / 2 > 0 ? i - a.sA / 2 : 0, i2 = i + a.sA / 2 < a.nA - 1 ? i + a.sA / 2 : a.nA - 1;
+    const int j1 = j - a.sR / 2 > 0 ? j - a.sR / 2 : 0, j2 = j + a.sR / 2 < a.nR - 1 ? j + a.sR / 2 : a.nR - 1;
+    unsigned ngood = 0;
+    float nLooksEff = 0.0f;
+    double meanA = 0.0, meanR = 0.0;
+    for (int ii = i1; ii <= i2; ii++)
+        for (int jj = j1; jj <= j2; jj++) {
+            const size_t q = (size_t)ii * a.nR + jj;
+            if (valid_pt(a.offR[q], a.offA[q])) {
+                ngood++;
+                nLooksEff += 1.0f;
+                meanA += (double)a.offA[q];
+                meanR += (double)a.offR[q];
+            }
+        }
+    if (((ngood > 1) || (a.sA == 1) || (a.sR == 1)) && a.offR[k] > kValidLim && a.sigmaA[k] > kValidLim) {
+        nLooksEff = (float)((double)nLooksEff > 1. ? (double)nLooksEff : 1.);
+        a.sigmaA[k] = (float)((double)a.sigmaA[k] / sqrt((double)nLooksEff));
+        a.sigmaR[k] = (float)((double)a.sigmaR[k] / sqrt((double)nLooksEff));
+        a.offRS[k] = (float)(meanR / (float)ngood);
+        a.offAS[k] = (float)(meanA / (float)ngood);
+    } else {
+        a.offRS[k] = kCulled;
+        a.offAS[k] = kCulled;
+    }
+}
+
+// cullLSData.c:36-57 (first pass): valid points and points with data.
+__global__ void cullls_count_kernel(const float* offR, const float* offA, const uint8_t* type, unsigned noDataMask,
+                                    long long n, unsigned long long* cnt)
+{
+    unsigned long long nv = 0, nd = 0;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+         p += (long long)gridDim.x * blockDim.x) {
+        nv += valid_pt(offR[p], offA[p]);
+        nd += (type[p] & noDataMask) == 0;
+    }
+    nv = __reduce_add_sync(0xffffffffu, (unsigned)nv);
+    nd = __reduce_add_sync(0xffffffffu, (unsigned)nd);
+    if ((threadIdx.x & 31) == 0) {
+        if (nv) atomicAdd(&cnt[0], nv);
+        if (nd) atomicAdd(&cnt[1], nd);
     }
 }
 
@@ -639,6 +719,63 @@ struct CullDev {
     uint8_t *type, *mask;
 };
 
+// What the passes read, from either entry point (cullst or cullls).
+struct CullJob {
+    int nR, nA, bR, bA, sR, sA, islandThresh, connectivity;
+    StRule rule;          // rule.slowType is set to the device type grid (cullls)
+    bool prepass;         // cullst: corr threshold and mask tests before the median pass
+    float corrThresh;
+    int singleMT;
+    double qvar;          // cullls stats: quantisation variance
+    bool lsSmooth;        // cullls smoothing
+};
+
+CullJob job_of(const sb_cull_params* p)
+{
+    CullJob j;
+    j.nR = p->nR; j.nA = p->nA; j.bR = p->bR; j.bA = p->bA; j.sR = p->sR; j.sA = p->sA;
+    j.islandThresh = p->islandThresh; j.connectivity = p->connectivity;
+    j.rule.nGood = p->nGood;
+    j.rule.maxR = p->maxR; j.rule.maxA = p->maxA;
+    j.rule.slowMaxR = p->maxR; j.rule.slowMaxA = p->maxA;
+    j.rule.slowType = nullptr;
+    j.rule.slowMask = 0;
+    j.rule.selfTest = false;
+    j.rule.selfLim = 0.0;
+    j.prepass = true;
+    j.corrThresh = p->corrThresh;
+    j.singleMT = p->singleMT;
+    j.qvar = 0.0;
+    j.lsSmooth = false;
+    return j;
+}
+
+// cullLSData.c:99-117: limits where every valid neighbour is slow-moving,
+// 40 m/yr over deltaT in pixels, at least 0.2; cullLSStats.c:147-148.
+CullJob job_of(const sb_cullls_params* p)
+{
+    CullJob j;
+    j.nR = p->nx; j.nA = p->ny; j.bR = p->boxSize; j.bA = p->boxSize; j.sR = p->sX; j.sA = p->sY;
+    j.islandThresh = p->islandThresh; j.connectivity = p->connectivity;
+    j.rule.nGood = p->nGood;
+    j.rule.maxR = p->maxX; j.rule.maxA = p->maxY;
+    double mx = 40.0 / 365. * p->deltaT, my = mx;
+    mx /= p->dx;
+    my /= p->dy;
+    j.rule.slowMaxR = mx > 0.2 ? mx : 0.2;
+    j.rule.slowMaxA = my > 0.2 ? my : 0.2;
+    j.rule.slowType = nullptr;
+    j.rule.slowMask = p->slowVelMask;
+    j.rule.selfTest = true;
+    j.rule.selfLim = p->noDataLimit;
+    j.prepass = false;
+    j.corrThresh = 0.0f;
+    j.singleMT = 0;
+    j.qvar = ((1.0 / p->nOver) * (1.0 / p->nOver)) / 12.;
+    j.lsSmooth = true;
+    return j;
+}
+
 int cull_check(sb_context* c, const sb_cull_params* p, const sb_cull_data* d)
 {
     if (!c) return SB_ERR_ARG;
@@ -725,10 +862,10 @@ int cull_stage_out(sb_context* c, const sb_cull_params* p, sb_cull_data* d, cons
 // after kMaxFixSteps steps (or the box is too large for the warp medians):
 // the caller then runs the wavefront kernel.
 constexpr int kMaxFixSteps = 48;
-int run_st_fixpoint(sb_context* c, const sb_cull_params* p, sb_cull_data* d, const CullDev* v, int nv, int* ctl)
+int run_st_fixpoint(sb_context* c, const CullJob& p, const CullDev* v, int nv, int* ctl, int64_t* nCulledOut)
 {
     if (nv > 4) return SB_ERR_UNSUPPORTED;
-    const long long n = (long long)p->nR * p->nA;
+    const long long n = (long long)p.nR * p.nA;
     cudaError_t e;
     uint8_t* fl = (uint8_t*)sb_ctx_buf(c, "c_fix", (size_t)n * 4, &e);
     if (!fl) return sb_ctx_fail(c, SB_ERR_NOMEM, "device allocation failed");
@@ -739,8 +876,8 @@ int run_st_fixpoint(sb_context* c, const sb_cull_params* p, sb_cull_data* d, con
     CKC(cudaMemsetAsync(C[0], 0, (size_t)n, s), "memset");
     FixArgs f;
     f.offR = v->offR; f.offA = v->offA;
-    f.nR = p->nR; f.nA = p->nA; f.bR = p->bR; f.bA = p->bA; f.nGood = p->nGood;
-    f.maxA = p->maxA; f.maxR = p->maxR;
+    f.nR = p.nR; f.nA = p.nA; f.bR = p.bR; f.bA = p.bA;
+    f.rule = p.rule;
     f.nChanged = nChanged;
     const int threads = 256;
     long long blocks = (n * 32 + threads - 1) / threads;
@@ -774,44 +911,47 @@ int run_st_fixpoint(sb_context* c, const sb_cull_params* p, sb_cull_data* d, con
             unsigned long long culled = 0;
             CKC(cudaMemcpyAsync(&culled, nCulled, sizeof(culled), cudaMemcpyDeviceToHost, s), "d2h");
             CKC(cudaStreamSynchronize(s), "cull_apply");
-            d->nCulled = (int64_t)culled;
+            *nCulledOut = (int64_t)culled;
             return SB_OK;
         }
     }
     return SB_ERR_UNSUPPORTED;
 }
 
-int run_st_data(sb_context* c, const sb_cull_params* p, sb_cull_data* d, const CullDev* v)
+int run_st_data(sb_context* c, const CullJob& p, const CullDev* v, int64_t* nCulledOut)
 {
-    const int n = p->nR * p->nA;
+    const int n = p.nR * p.nA;
     cudaError_t e;
     int* ctl = (int*)sb_ctx_buf(c, "c_ctl", sizeof(int) * 4 + sizeof(unsigned long long) * 2, &e);
-    int* progress = (int*)sb_ctx_buf(c, "c_progress", sizeof(int) * (size_t)p->nA, &e);
+    int* progress = (int*)sb_ctx_buf(c, "c_progress", sizeof(int) * (size_t)p.nA, &e);
     if (!ctl || !progress) return sb_ctx_fail(c, SB_ERR_NOMEM, "device allocation failed");
     CullArgs a;
     a.offR = v->offR; a.offA = v->offA; a.corr = v->corr; a.type = v->type; a.mask = v->mask;
-    a.nR = p->nR; a.nA = p->nA; a.bR = p->bR; a.bA = p->bA; a.nGood = p->nGood;
-    a.maxA = p->maxA; a.maxR = p->maxR; a.corrThresh = p->corrThresh; a.singleMT = p->singleMT;
+    a.nR = p.nR; a.nA = p.nA; a.bR = p.bR; a.bA = p.bA;
+    a.rule = p.rule;
+    a.corrThresh = p.corrThresh; a.singleMT = p.singleMT;
     a.rowCounter = ctl;
     a.errFlag = ctl + 1;
     a.nCulled = (unsigned long long*)(ctl + 4);
     a.progress = progress;
     cudaStream_t s = c->stream;
     CKC(cudaMemsetAsync(ctl, 0, sizeof(int) * 4 + sizeof(unsigned long long) * 2, s), "memset");
-    CKC(cudaMemsetAsync(progress, 0, sizeof(int) * (size_t)p->nA, s), "memset");
-    cull_prepass_kernel<<<(n + 255) / 256, 256, 0, s>>>(a);
-    CKC(cudaGetLastError(), "cull_prepass");
-    c->launches++;
-    const int box = (p->bR / 2 * 2 + 1) * (p->bA / 2 * 2 + 1);
+    CKC(cudaMemsetAsync(progress, 0, sizeof(int) * (size_t)p.nA, s), "memset");
+    if (p.prepass) {
+        cull_prepass_kernel<<<(n + 255) / 256, 256, 0, s>>>(a);
+        CKC(cudaGetLastError(), "cull_prepass");
+        c->launches++;
+    }
+    const int box = (p.bR / 2 * 2 + 1) * (p.bA / 2 * 2 + 1);
     const int nv = (box + 31) / 32;
     // parallel fixpoint first (exact when it converges), the wavefront if not
     {
-        int rc = run_st_fixpoint(c, p, d, v, nv, ctl);
+        int rc = run_st_fixpoint(c, p, v, nv, ctl, nCulledOut);
         if (rc != SB_ERR_UNSUPPORTED) return rc;
     }
     // one warp per row in flight; enough warps for the wavefront depth
     int warps = c->numSM * 32;
-    if (warps > p->nA) warps = p->nA;
+    if (warps > p.nA) warps = p.nA;
     const int threads = 128, blocks = (warps * 32 + threads - 1) / threads;
     const long long spinLimit = 1LL << 26;  // ~4 s of 64 ns naps per wait
     switch (nv) {
@@ -832,31 +972,34 @@ int run_st_data(sb_context* c, const sb_cull_params* p, sb_cull_data* d, const C
     CKC(cudaMemcpyAsync(&culled, ctl + 4, sizeof(culled), cudaMemcpyDeviceToHost, s), "d2h");
     CKC(cudaStreamSynchronize(s), "cull_median");
     if (hostCtl[1]) return sb_ctx_fail(c, SB_ERR_TIMEOUT, "cullSTData wavefront wait timed out");
-    d->nCulled = (int64_t)culled;
+    *nCulledOut = (int64_t)culled;
     return SB_OK;
 }
 
-int run_stats(sb_context* c, const sb_cull_params* p, const CullDev* v)
+int run_stats(sb_context* c, const CullJob& p, const CullDev* v)
 {
-    const int n = p->nR * p->nA;
-    StatsArgs a{v->offR, v->offA, v->sigmaR, v->sigmaA, p->nR, p->nA};
+    const int n = p.nR * p.nA;
+    StatsArgs a{v->offR, v->offA, v->sigmaR, v->sigmaA, p.nR, p.nA, p.qvar};
     cull_stats_kernel<<<(n + 127) / 128, 128, 0, c->stream>>>(a);
     c->launches++;
     return sb_ctx_cuda(c, cudaGetLastError(), "cull_stats");
 }
 
-int run_smooth(sb_context* c, const sb_cull_params* p, const CullDev* v)
+int run_smooth(sb_context* c, const CullJob& p, const CullDev* v)
 {
-    const int n = p->nR * p->nA;
-    SmoothArgs a{v->offR, v->offA, v->type, v->sigmaR, v->sigmaA, v->offRS, v->offAS, p->nR, p->nA, p->sR, p->sA};
-    cull_smooth_kernel<<<(n + 127) / 128, 128, 0, c->stream>>>(a);
+    const int n = p.nR * p.nA;
+    SmoothArgs a{v->offR, v->offA, v->type, v->sigmaR, v->sigmaA, v->offRS, v->offAS, p.nR, p.nA, p.sR, p.sA};
+    if (p.lsSmooth)
+        cullls_smooth_kernel<<<(n + 127) / 128, 128, 0, c->stream>>>(a);
+    else
+        cull_smooth_kernel<<<(n + 127) / 128, 128, 0, c->stream>>>(a);
     c->launches++;
     return sb_ctx_cuda(c, cudaGetLastError(), "cull_smooth");
 }
 
-int run_islands(sb_context* c, const sb_cull_params* p, sb_cull_data* d, const CullDev* v)
+int run_islands(sb_context* c, const CullJob& p, const CullDev* v, int64_t* nIslands, int64_t* nIslandPoints)
 {
-    const int n = p->nR * p->nA;
+    const int n = p.nR * p.nA;
     cudaError_t e;
     int* ws = (int*)sb_ctx_buf(c, "c_isl", sizeof(int) * (size_t)n * 5 + 64, &e);
     unsigned long long* cntd = (unsigned long long*)sb_ctx_buf(c, "c_isl_cnt", 4 * sizeof(unsigned long long), &e);
@@ -871,10 +1014,10 @@ int run_islands(sb_context* c, const sb_cull_params* p, sb_cull_data* d, const C
     a.maxY = ws + 4 * (size_t)n;
     a.lastRoot = ws + 5 * (size_t)n;
     a.counts = cntd;
-    a.nR = p->nR;
-    a.nA = p->nA;
-    a.conn8 = p->connectivity != 4;
-    a.thresh = p->islandThresh;
+    a.nR = p.nR;
+    a.nA = p.nA;
+    a.conn8 = p.connectivity != 4;
+    a.thresh = p.islandThresh;
     cudaStream_t s = c->stream;
     CKC(cudaMemsetAsync(a.lastRoot, 0xff, sizeof(int), s), "memset");
     CKC(cudaMemsetAsync(a.counts, 0, 2 * sizeof(unsigned long long), s), "memset");
@@ -888,34 +1031,34 @@ int run_islands(sb_context* c, const sb_cull_params* p, sb_cull_data* d, const C
     unsigned long long cnt[2];
     CKC(cudaMemcpyAsync(cnt, a.counts, sizeof(cnt), cudaMemcpyDeviceToHost, s), "d2h");
     CKC(cudaStreamSynchronize(s), "cull_islands");
-    d->nIslands = (int64_t)cnt[0];
-    d->nIslandPoints = (int64_t)cnt[1];
+    *nIslands = (int64_t)cnt[0];
+    *nIslandPoints = (int64_t)cnt[1];
     return SB_OK;
 }
 
-int run_sim(sb_context* c, const sb_cull_params* p, const CullDev* v, float sign)
+int run_sim(sb_context* c, const CullJob& p, const CullDev* v, float sign)
 {
-    const int n = p->nR * p->nA;
+    const int n = p.nR * p.nA;
     cull_sim_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(v->offR, v->offA, v->simR, v->simA, n, sign);
     c->launches++;
     return sb_ctx_cuda(c, cudaGetLastError(), "cull_sim");
 }
 
-template <typename F>
-int cull_entry(sb_context* c, const sb_cull_params* p, sb_cull_data* d, F body)
+// Stage in, run the passes, stage out, with the context's four timing events.
+template <typename In, typename F, typename Out>
+int cull_run(sb_context* c, In stageIn, F body, Out stageOut)
 {
-    int rc = cull_check(c, p, d);
-    if (rc != SB_OK) return rc;
+    int rc;
     c->err.clear();
     c->launches = 0;
     CKC(cudaSetDevice(c->device), "cudaSetDevice");
     cudaEventRecord(c->ev[0], c->stream);
     CullDev v;
-    if ((rc = cull_stage_in(c, p, d, &v)) != SB_OK) return rc;
+    if ((rc = stageIn(&v)) != SB_OK) return rc;
     cudaEventRecord(c->ev[1], c->stream);
     if ((rc = body(v)) != SB_OK) return rc;
     cudaEventRecord(c->ev[2], c->stream);
-    if ((rc = cull_stage_out(c, p, d, &v)) != SB_OK) return rc;
+    if ((rc = stageOut(&v)) != SB_OK) return rc;
     cudaEventRecord(c->ev[3], c->stream);
     CKC(cudaStreamSynchronize(c->stream), "cull");
     cudaEventElapsedTime(&c->timing[0], c->ev[0], c->ev[3]);
@@ -925,40 +1068,153 @@ int cull_entry(sb_context* c, const sb_cull_params* p, sb_cull_data* d, F body)
     return SB_OK;
 }
 
+template <typename F>
+int cull_entry(sb_context* c, const sb_cull_params* p, sb_cull_data* d, F body)
+{
+    int rc = cull_check(c, p, d);
+    if (rc != SB_OK) return rc;
+    return cull_run(
+        c, [&](CullDev* v) { return cull_stage_in(c, p, d, v); }, body,
+        [&](const CullDev* v) { return cull_stage_out(c, p, d, v); });
+}
+
+int cullls_check(sb_context* c, const sb_cullls_params* p, const sb_cullls_data* d)
+{
+    if (!c) return SB_ERR_ARG;
+    if (!p || !d) return sb_ctx_fail(c, SB_ERR_ARG, "null params or data");
+    if (p->nx <= 0 || p->ny <= 0) return sb_ctx_fail(c, SB_ERR_ARG, "empty grid");
+    if ((long long)p->nx * p->ny > (1LL << 30)) return sb_ctx_fail(c, SB_ERR_ARG, "grid too large");
+    if (!d->X || !d->Y || !d->type) return sb_ctx_fail(c, SB_ERR_ARG, "null input grid");
+    if (p->boxSize < 0 || (p->boxSize / 2 * 2 + 1) * (p->boxSize / 2 * 2 + 1) > 32 * 32)
+        return sb_ctx_fail(c, SB_ERR_UNSUPPORTED, "cull box larger than 32 x 32");
+    if (!(p->nOver > 0.0)) return sb_ctx_fail(c, SB_ERR_ARG, "nOver (lstrack's NOVER) must be positive");
+    if (!(p->dx > 0.0) || !(p->dy > 0.0)) return sb_ctx_fail(c, SB_ERR_ARG, "pixel sizes dx, dy must be positive");
+    return SB_OK;
+}
+
+int cullls_stage_in(sb_context* c, const sb_cullls_params* p, sb_cullls_data* d, CullDev* v)
+{
+    const size_t n = (size_t)p->nx * p->ny, fb = n * sizeof(float);
+    cudaError_t e;
+    *v = CullDev{};
+    if (d->onDevice) {
+        v->offR = d->X; v->offA = d->Y; v->type = (uint8_t*)d->type;
+        v->offRS = d->XS; v->offAS = d->YS; v->sigmaR = d->sigmaX; v->sigmaA = d->sigmaY;
+    } else {
+        v->offR = (float*)sb_ctx_buf(c, "c_offR", fb, &e);
+        v->offA = (float*)sb_ctx_buf(c, "c_offA", fb, &e);
+        v->type = (uint8_t*)sb_ctx_buf(c, "c_type", n, &e);
+        if (!v->offR || !v->offA || !v->type) return sb_ctx_fail(c, SB_ERR_NOMEM, "device allocation failed");
+        CKC(cudaMemcpyAsync(v->offR, d->X, fb, cudaMemcpyHostToDevice, c->stream), "h2d");
+        CKC(cudaMemcpyAsync(v->offA, d->Y, fb, cudaMemcpyHostToDevice, c->stream), "h2d");
+        CKC(cudaMemcpyAsync(v->type, d->type, n, cudaMemcpyHostToDevice, c->stream), "h2d");
+    }
+    if (!d->onDevice || !v->offRS) v->offRS = (float*)sb_ctx_buf(c, "c_offRS", fb, &e);
+    if (!d->onDevice || !v->offAS) v->offAS = (float*)sb_ctx_buf(c, "c_offAS", fb, &e);
+    if (!d->onDevice || !v->sigmaR) v->sigmaR = (float*)sb_ctx_buf(c, "c_sigmaR", fb, &e);
+    if (!d->onDevice || !v->sigmaA) v->sigmaA = (float*)sb_ctx_buf(c, "c_sigmaA", fb, &e);
+    if (!v->offRS || !v->offAS || !v->sigmaR || !v->sigmaA)
+        return sb_ctx_fail(c, SB_ERR_NOMEM, "device allocation failed");
+    return SB_OK;
+}
+
+int cullls_stage_out(sb_context* c, const sb_cullls_params* p, sb_cullls_data* d, const CullDev* v)
+{
+    if (d->onDevice) return SB_OK;
+    const size_t fb = (size_t)p->nx * p->ny * sizeof(float);
+    cudaStream_t s = c->stream;
+    CKC(cudaMemcpyAsync(d->X, v->offR, fb, cudaMemcpyDeviceToHost, s), "d2h");
+    CKC(cudaMemcpyAsync(d->Y, v->offA, fb, cudaMemcpyDeviceToHost, s), "d2h");
+    if (d->XS) CKC(cudaMemcpyAsync(d->XS, v->offRS, fb, cudaMemcpyDeviceToHost, s), "d2h");
+    if (d->YS) CKC(cudaMemcpyAsync(d->YS, v->offAS, fb, cudaMemcpyDeviceToHost, s), "d2h");
+    if (d->sigmaX) CKC(cudaMemcpyAsync(d->sigmaX, v->sigmaR, fb, cudaMemcpyDeviceToHost, s), "d2h");
+    if (d->sigmaY) CKC(cudaMemcpyAsync(d->sigmaY, v->sigmaA, fb, cudaMemcpyDeviceToHost, s), "d2h");
+    return SB_OK;
+}
+
+// nAttempt / nMatch of the first cullLSData pass (cullLSData.c:36-57).
+int run_ls_counts(sb_context* c, const sb_cullls_params* p, const CullDev* v, sb_cullls_data* d)
+{
+    const long long n = (long long)p->nx * p->ny;
+    cudaError_t e;
+    unsigned long long* cnt = (unsigned long long*)sb_ctx_buf(c, "c_lscnt", 2 * sizeof(unsigned long long), &e);
+    if (!cnt) return sb_ctx_fail(c, SB_ERR_NOMEM, "device allocation failed");
+    cudaStream_t s = c->stream;
+    CKC(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned long long), s), "memset");
+    long long blocks = (n + 255) / 256;
+    if (blocks > (long long)c->numSM * 16) blocks = (long long)c->numSM * 16;
+    cullls_count_kernel<<<(int)blocks, 256, 0, s>>>(v->offR, v->offA, v->type, p->noDataMask, n, cnt);
+    CKC(cudaGetLastError(), "cullls_count");
+    c->launches++;
+    unsigned long long h[2];
+    CKC(cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, s), "d2h");
+    CKC(cudaStreamSynchronize(s), "cullls_count");
+    d->nMatch = (int64_t)h[0];
+    d->nAttempt = (int64_t)h[1];
+    return SB_OK;
+}
+
 }  // namespace
 
 extern "C" int sb_cull(sb_context* c, const sb_cull_params* p, sb_cull_data* d)
 {
     return cull_entry(c, p, d, [&](const CullDev& v) {
         int rc;
-        if (p->useSim && (rc = run_sim(c, p, &v, -1.0f)) != SB_OK) return rc;
+        const CullJob j = job_of(p);
+        if (p->useSim && (rc = run_sim(c, j, &v, -1.0f)) != SB_OK) return rc;
         const int passes = p->nCullPasses > 0 ? p->nCullPasses : 3;
         for (int k = 0; k < passes; ++k)
-            if ((rc = run_st_data(c, p, d, &v)) != SB_OK) return rc;
-        if ((rc = run_stats(c, p, &v)) != SB_OK) return rc;
-        if (p->useSim && (rc = run_sim(c, p, &v, 1.0f)) != SB_OK) return rc;
-        if ((rc = run_smooth(c, p, &v)) != SB_OK) return rc;
-        if (p->islandThresh > 0 && (rc = run_islands(c, p, d, &v)) != SB_OK) return rc;
+            if ((rc = run_st_data(c, j, &v, &d->nCulled)) != SB_OK) return rc;
+        if ((rc = run_stats(c, j, &v)) != SB_OK) return rc;
+        if (p->useSim && (rc = run_sim(c, j, &v, 1.0f)) != SB_OK) return rc;
+        if ((rc = run_smooth(c, j, &v)) != SB_OK) return rc;
+        if (p->islandThresh > 0 && (rc = run_islands(c, j, &v, &d->nIslands, &d->nIslandPoints)) != SB_OK)
+            return rc;
         return SB_OK;
     });
 }
 
 extern "C" int sb_cull_st_data(sb_context* c, const sb_cull_params* p, sb_cull_data* d)
 {
-    return cull_entry(c, p, d, [&](const CullDev& v) { return run_st_data(c, p, d, &v); });
+    return cull_entry(c, p, d, [&](const CullDev& v) { return run_st_data(c, job_of(p), &v, &d->nCulled); });
 }
 
 extern "C" int sb_cull_stats(sb_context* c, const sb_cull_params* p, sb_cull_data* d)
 {
-    return cull_entry(c, p, d, [&](const CullDev& v) { return run_stats(c, p, &v); });
+    return cull_entry(c, p, d, [&](const CullDev& v) { return run_stats(c, job_of(p), &v); });
 }
 
 extern "C" int sb_cull_smooth(sb_context* c, const sb_cull_params* p, sb_cull_data* d)
 {
-    return cull_entry(c, p, d, [&](const CullDev& v) { return run_smooth(c, p, &v); });
+    return cull_entry(c, p, d, [&](const CullDev& v) { return run_smooth(c, job_of(p), &v); });
 }
 
 extern "C" int sb_cull_islands(sb_context* c, const sb_cull_params* p, sb_cull_data* d)
 {
-    return cull_entry(c, p, d, [&](const CullDev& v) { return run_islands(c, p, d, &v); });
+    return cull_entry(
+        c, p, d, [&](const CullDev& v) { return run_islands(c, job_of(p), &v, &d->nIslands, &d->nIslandPoints); });
+}
+
+extern "C" int sb_cullls(sb_context* c, const sb_cullls_params* p, sb_cullls_data* d)
+{
+    int rc = cullls_check(c, p, d);
+    if (rc != SB_OK) return rc;
+    return cull_run(
+        c, [&](CullDev* v) { return cullls_stage_in(c, p, d, v); },
+        [&](const CullDev& v) {
+            int r;
+            CullJob j = job_of(p);
+            j.rule.slowType = v.type;
+            if ((r = run_ls_counts(c, p, &v, d)) != SB_OK) return r;
+            const int passes = p->nCullPasses > 0 ? p->nCullPasses : 3;
+            for (int k = 0; k < passes; ++k)
+                if ((r = run_st_data(c, j, &v, &d->nCulled)) != SB_OK) return r;
+            if ((r = run_stats(c, j, &v)) != SB_OK) return r;
+            if ((r = run_smooth(c, j, &v)) != SB_OK) return r;
+            d->nIslands = d->nIslandPoints = 0;
+            if (p->islandThresh > 0 && (r = run_islands(c, j, &v, &d->nIslands, &d->nIslandPoints)) != SB_OK)
+                return r;
+            return SB_OK;
+        },
+        [&](const CullDev* v) { return cullls_stage_out(c, p, d, v); });
 }

@@ -95,3 +95,56 @@ def write_offsets(base, offR, offA, corr, mt, r0, a0, deltaR, deltaA):
     np.ascontiguousarray(mt, np.uint8).tofile(base + ".mt")
     with open(base + ".dat", "w") as f:
         f.write(f"{r0} {a0} {nr} {na} {deltaR} {deltaA}\n")
+
+
+def write_ls_culled(match_file, res, params, meta):
+    """writeLSCulledOffsets (Cullls/cullls.c:61-161): <match_file>.cull.dx,
+    .cull.dy, .cull.sx, .cull.sy (big-endian float32), .cull.mtype (uint8) and
+    the .cull.dat summary.  res: a cullls result (XS, YS, sigmaX, sigmaY,
+    type, nMatch, nAttempt); params: its CullLSParams (noDataLimit); meta: the
+    matchResult/lsFit fields the summary prints (fileEarly, fileLate, x0, y0,
+    dx, dy, stepX, stepY, slowFlag, proj, jdEarly, jdLate).  Returns the
+    summary's (nGoodPts, sigmaXAvg, sigmaYAvg)."""
+    XS, YS = res["XS"], res["YS"]
+    ny, nx = XS.shape
+    good = (XS.astype(np.float64) > params.noDataLimit) & (YS.astype(np.float64) > params.noDataLimit)
+    n_good = int(good.sum())
+    # float products summed in double in raster order, as the reference's loop
+    sx = res["sigmaX"][good].astype(np.float32)
+    sy = res["sigmaY"][good].astype(np.float32)
+    acc_x = float(np.cumsum((sx * sx).astype(np.float64))[-1]) if n_good else 0.0
+    acc_y = float(np.cumsum((sy * sy).astype(np.float64))[-1]) if n_good else 0.0
+    sig_x = float(np.sqrt(acc_x / max(n_good, 1)))
+    sig_y = float(np.sqrt(acc_y / max(n_good, 1)))
+    for ext, arr in ((".cull.dx", XS), (".cull.dy", YS), (".cull.sx", res["sigmaX"]), (".cull.sy", res["sigmaY"])):
+        np.ascontiguousarray(arr, ">f4").tofile(match_file + ext)
+    np.ascontiguousarray(res["type"], np.uint8).tofile(match_file + ".cull.mtype")
+    att = max(int(res["nAttempt"]), 1)
+    success = float(np.float32(res["nMatch"]) / np.float32(att)) * 100.0
+    culled = float(np.float32(n_good) / np.float32(att)) * 100.0
+    m = meta
+    lines = [
+        f"fileEarly = {m['fileEarly']}",
+        f"fileLate = {m['fileLate']}",
+        f"x0 = {m['x0']:11.2f}",
+        f"y0 = {m['y0']:11.2f}",
+        f"dx = {m['dx']:10.5f}",
+        f"dy = {m['dy']:10.5f}",
+        f"stepY = {int(m['stepX'])}",  # the reference prints stepX under "stepY" and vice versa
+        f"stepX = {int(m['stepY'])}",
+        f"nx = {nx:9d}",
+        f"ny = {ny:9d}",
+        f"slowFlag = {int(m['slowFlag']):9d}",
+        f"EPSG = {int(m['proj']):9d}",
+        f"earlyImageJD = {m['jdEarly']:10f}",
+        f"lateImageJD = {m['jdLate']:10f}",
+        f"IntervalBetweenImages = {int(m['jdLate'] - m['jdEarly']):5d}",
+        f"Success_rate_for_attempted_matches(%) =  {success:7.2f} ",
+        f"Culled_rate_for_attempted_matches(%) =  {culled:7.2f} ",
+        f"Mean_sigmaX = {sig_x:11.3f}",
+        f"Mean_sigmaY = {sig_y:11.3f}",
+        "& ",
+    ]
+    with open(match_file + ".cull.dat", "w") as f:
+        f.write("\n".join(lines) + "\n")
+    return n_good, sig_x, sig_y

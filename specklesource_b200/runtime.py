@@ -34,6 +34,7 @@ SIGNATURES = {
     "sb_cull_stats": (C.c_int, [_P, C.POINTER(abi.SbCullParams), C.POINTER(abi.SbCullData)]),
     "sb_cull_smooth": (C.c_int, [_P, C.POINTER(abi.SbCullParams), C.POINTER(abi.SbCullData)]),
     "sb_cull_islands": (C.c_int, [_P, C.POINTER(abi.SbCullParams), C.POINTER(abi.SbCullData)]),
+    "sb_cullls": (C.c_int, [_P, C.POINTER(abi.SbCulllsParams), C.POINTER(abi.SbCulllsData)]),
     "sb_amp_match_noalloc": (C.c_int, [_P, _P, _P, C.c_int32, C.c_int32, _P, _P, _P, _P, _P]),
 }
 
@@ -188,6 +189,15 @@ class Context:
         d["nCulled"] = cd.nCulled
         d["nIslands"] = cd.nIslands
         d["nIslandPoints"] = cd.nIslandPoints
+        return d
+
+    def cullls(self, params, X, Y, mtype):
+        """cullls pipeline (Cullls/cullls.c:23-56) on the GPU."""
+        d, cd = abi.cullls_data(X, Y, mtype)
+        cp = params.to_c()
+        self._check(self.lib.sb_cullls(self.h, C.byref(cp), C.byref(cd)))
+        for k in ("nAttempt", "nMatch", "nCulled", "nIslands", "nIslandPoints"):
+            d[k] = getattr(cd, k)
         return d
 
 

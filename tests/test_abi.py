@@ -63,6 +63,8 @@ _STRUCTS = {
     "sb_track_result": abi.SbTrackResult,
     "sb_cull_params": abi.SbCullParams,
     "sb_cull_data": abi.SbCullData,
+    "sb_cullls_params": abi.SbCulllsParams,
+    "sb_cullls_data": abi.SbCulllsData,
 }
 
 

@@ -95,3 +95,60 @@ def test_cull_large_grid_keep_mask(ctx):
     _check(g, o)
     print("cull 700x993:", t)
     assert o["nIslands"] > 0
+
+
+# ---------------------------------------------------------------- cullls
+
+SLOW, NODATA_BIT = 0x10, 0x40  # stand-ins for lstrack.h's SLOWVEL / NODATATOUSE
+
+
+def _ls_inputs(nA, nR, seed):
+    X, Y, _, mt = offsets_field(nA, nR, seed)
+    rng = np.random.default_rng(seed + 100)
+    yy, xx = np.mgrid[0:nA, 0:nR]
+    t = np.where((xx - nR / 3) ** 2 + (yy - nA / 2) ** 2 < (nA / 3) ** 2, SLOW, 0)  # a slow-moving disc
+    t = t | np.where(rng.random((nA, nR)) < 0.05, NODATA_BIT, 0) | (mt & 3)
+    return X, Y, t.astype(np.uint8)
+
+
+def _check_ls(g, o):
+    for k in ("X", "Y"):
+        assert _same(g[k], o[k]), f"{k} differs at {np.argwhere(~((g[k] == o[k]) | (np.isnan(g[k]) & np.isnan(o[k]))))[:5]}"
+    for k in ("XS", "YS"):
+        vg, vo = g[k] > -1.9e9, o[k] > -1.9e9
+        assert np.array_equal(vg, vo), f"{k} keep mask differs"
+        assert np.allclose(g[k][vo], o[k][vo], rtol=1e-6, atol=1e-6)
+    for k in ("sigmaX", "sigmaY"):
+        vg, vo = g[k] > -1.9e9, o[k] > -1.9e9
+        assert np.array_equal(vg, vo), f"{k} validity differs"
+        assert np.allclose(g[k][vo], o[k][vo], rtol=2e-3, atol=1e-5)
+    for k in ("nAttempt", "nMatch", "nCulled", "nIslands", "nIslandPoints"):
+        assert g[k] == o[k], k
+
+
+@pytest.mark.parametrize("kw", [
+    dict(islandThresh=6),                                                   # cullls defaults, islands
+    dict(boxSize=5, nGood=8, sX=1, sY=5, noDataLimit=-3.0, connectivity=4, islandThresh=3),
+    dict(boxSize=13, nGood=40, deltaT=24.0, dx=30.0, dy=30.0),              # box above 128 values: the wavefront kernel
+])
+def test_cullls_matches_oracle(ctx, kw):
+    nA, nR = 150, 230
+    X, Y, t = _ls_inputs(nA, nR, 11)
+    base = dict(nx=nR, ny=nA, deltaT=365.0, dx=15.0, dy=15.0, nOver=10.0, slowVelMask=SLOW, noDataMask=NODATA_BIT)
+    base.update(kw)
+    p = abi.CullLSParams(**base)
+    g = ctx.cullls(p, X, Y, t)
+    o = oracle.cullls(p, X, Y, t)
+    _check_ls(g, o)
+    assert o["nCulled"] > 0 and o["nMatch"] > o["nCulled"]
+
+
+def test_cullls_large_grid(ctx):
+    nA, nR = 700, 993
+    X, Y, t = _ls_inputs(nA, nR, 12)
+    p = abi.CullLSParams(nx=nR, ny=nA, deltaT=48.0, dx=15.0, dy=15.0, nOver=10.0, slowVelMask=SLOW,
+                         noDataMask=NODATA_BIT, islandThresh=10)
+    g = ctx.cullls(p, X, Y, t)
+    o = oracle.cullls(p, X, Y, t)
+    _check_ls(g, o)
+    assert o["nIslands"] > 0

@@ -273,3 +273,87 @@ def test_gauss_fit_recovers_shift(dr, da):
         f = oracle.strack(p, z.astype(np.complex64), z2.astype(np.complex64), precision="f32")
         assert np.array_equal(f["offR"], o["offR"]) and np.array_equal(f["offA"], o["offA"])
 
+
+
+# ---------------------------------------------------------------- cullls
+
+SLOW, NODATA_BIT = 0x10, 0x40  # stand-ins for lstrack.h's SLOWVEL / NODATATOUSE
+
+
+def _ls_params(**kw):
+    base = dict(nx=40, ny=30, deltaT=365.0, dx=15.0, dy=15.0, nOver=10.0, slowVelMask=SLOW,
+                noDataMask=NODATA_BIT)
+    base.update(kw)
+    return abi.CullLSParams(**base)
+
+
+def test_cullls_slow_flow_limits():
+    """cullLSData.c:99-117: where every valid box point is slow-moving the
+    limits are 40 m/yr * deltaT / pixel size (here 2.67 px), not maxX/maxY."""
+    X, Y, _, _ = _grid()
+    X[10, 10] += 1.5
+    slow = np.full(X.shape, SLOW, np.uint8)
+    d = oracle.cullls(_ls_params(), X, Y, slow)
+    assert d["X"][10, 10] > -LARGE  # 1.5 px within the slow limit
+    d = oracle.cullls(_ls_params(), X, Y, np.zeros(X.shape, np.uint8))
+    assert d["X"][10, 10] == -LARGE  # above maxX = 0.75
+    mixed = slow.copy()
+    mixed[13, 13] = 0  # one fast point in the 9x9 box: the normal limits
+    d = oracle.cullls(_ls_params(), X, Y, mixed)
+    assert d["X"][10, 10] == -LARGE
+    # a year over 1 km pixels: 0.04 px, floored at 0.2
+    X2, Y2, _, _ = _grid()
+    X2[10, 10] += 0.3
+    assert oracle.cullls(_ls_params(dx=1000.0, dy=1000.0), X2, Y2, slow)["X"][10, 10] == -LARGE
+    assert oracle.cullls(_ls_params(dx=1000.0, dy=1000.0), X2, Y2, 0 * slow)["X"][10, 10] > -LARGE
+
+
+def test_cullls_nodata_gate_and_counts():
+    X, Y, _, _ = _grid()
+    X[3, 3] = -LARGE
+    Y[3, 3] = -LARGE
+    mt = np.zeros(X.shape, np.uint8)
+    mt[0, :5] = NODATA_BIT
+    Y[20, 20] = -1.5  # below the NODATA + 1 limit set next
+    d = oracle.cullls(_ls_params(noDataLimit=-1.0, maxY=5.0), X, Y, mt)
+    assert d["nMatch"] == 40 * 30 - 1 and d["nAttempt"] == 40 * 30 - 5
+    assert d["X"][20, 20] == -LARGE
+
+
+def test_cullls_stats_quantisation_and_plain_smoothing():
+    """On an exact plane the stats see only the 1e-5 floor plus (1/NOVER)^2/12
+    (cullLSStats.c:147-148); the smoothing is the unweighted 3x3 mean and
+    divides the sigmas by sqrt(9)."""
+    ny, nx = 30, 40
+    yy, xx = np.mgrid[0:ny, 0:nx]
+    X = (0.5 + 0.01 * xx + 0.02 * yy).astype(np.float32)
+    Y = (-0.2 + 0.005 * xx).astype(np.float32)
+    d = oracle.cullls(_ls_params(nOver=10.0), X, Y, np.zeros((ny, nx), np.uint8))
+    s = np.sqrt(np.float32(1e-5) + (0.1 * 0.1) / 12.0) / 3.0
+    assert d["sigmaX"][15, 20] == pytest.approx(s, rel=1e-5)
+    assert d["sigmaY"][15, 20] == pytest.approx(s, rel=1e-5)
+    assert d["XS"][15, 20] == pytest.approx(float(X[14:17, 19:22].astype(np.float64).mean()), rel=1e-6)
+    assert d["YS"][0, 0] == pytest.approx(float(Y[0:2, 0:2].astype(np.float64).mean()), rel=1e-6)
+
+
+def test_cullls_writer(tmp_path):
+    """writeLSCulledOffsets: big-endian grids and the .cull.dat summary."""
+    from specklesource_b200 import files
+    X, Y, _, _ = _grid()
+    X[10, 10] += 3.0
+    mt = np.full(X.shape, 1, np.uint8)
+    mt[0, :4] |= NODATA_BIT
+    p = _ls_params()
+    d = oracle.cullls(p, X, Y, mt)
+    meta = dict(fileEarly="a.tif", fileLate="b.tif", x0=-100000.0, y0=250000.0, dx=15.0, dy=15.0, stepX=16,
+                stepY=8, slowFlag=1, proj=3413, jdEarly=2459000.5, jdLate=2459016.5)
+    root = str(tmp_path / "match")
+    n_good, sx, sy = files.write_ls_culled(root, d, p, meta)
+    assert n_good == int(((d["XS"] > -1.9e9) & (d["YS"] > -1.9e9)).sum())
+    assert np.array_equal(np.fromfile(root + ".cull.dx", ">f4").reshape(X.shape), d["XS"])
+    assert np.array_equal(np.fromfile(root + ".cull.sy", ">f4").reshape(X.shape), d["sigmaY"])
+    txt = open(root + ".cull.dat").read().splitlines()
+    assert txt[6] == "stepY = 16" and txt[7] == "stepX = 8"
+    assert txt[14] == "IntervalBetweenImages =    16"
+    assert txt[15] == f"Success_rate_for_attempted_matches(%) =  {100.0 * 1200 / 1196:7.2f} "
+    assert txt[-1] == "& "
