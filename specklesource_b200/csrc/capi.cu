@@ -686,18 +686,43 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
             a.list = dlist2;
         }
         const int nBand = bands.nb > 1 ? bands.nb : 1;
+        // peak hand-off buffer: list chunks of at most kPeakChunk patches, each
+        // launched as complex kernel + peak kernel (-gauss keeps the fit in
+        // the complex kernel)
+        constexpr int kPeakChunk = 1 << 19;
+        PeakJob* dpeak = nullptr;
+        if (!p->gaussFlag) {
+            const size_t pc = nC < kPeakChunk ? (size_t)nC : (size_t)kPeakChunk;
+            dpeak = (PeakJob*)sb_ctx_buf(c, "peakjob", pc * sizeof(PeakJob), &e);
+            if (!dpeak) return sb_ctx_fail(c, SB_ERR_NOMEM, "device allocation failed");
+        }
         cudaEventRecord(c->sev[0], c->stream);
         for (int k = 0; k < nBand; ++k) {
-            const int cnt = bandOff[k + 1] - bandOff[k];
-            if (cnt == 0) continue;
+            if (bandOff[k + 1] == bandOff[k]) continue;
             CK(cudaStreamWaitEvent(c->stream, c->chunkEv[k], 0), "wait band");
-            CmplxArgs ak = a;
-            ak.list = a.list + bandOff[k];
-            ak.fit = dfit + bandOff[k];
-            ak.nList = cnt;
-            const int nCta = c->numSM * bpsm < cnt ? c->numSM * bpsm : cnt;
-            CK(launch_strack_cmplx(W, ak, nCta, c->stream), "strack_cmplx");
-            c->launches++;
+            for (int off = bandOff[k]; off < bandOff[k + 1]; off += kPeakChunk) {
+                const int cnt = bandOff[k + 1] - off < kPeakChunk ? bandOff[k + 1] - off : kPeakChunk;
+                CmplxArgs ak = a;
+                ak.list = a.list + off;
+                ak.fit = dfit + off;
+                ak.nList = cnt;
+                ak.peak = dpeak;
+                const int nCta = c->numSM * bpsm < cnt ? c->numSM * bpsm : cnt;
+                CK(launch_strack_cmplx(W, ak, nCta, c->stream), "strack_cmplx");
+                c->launches++;
+                if (dpeak) {
+                    PeakArgs pk;
+                    pk.peak = dpeak;
+                    pk.nList = cnt;
+                    pk.W = W;
+                    pk.hanCorr = a.hanCorr;
+                    pk.osD = a.osD;
+                    pk.rec = drec;
+                    pk.fit = dfit + off;
+                    CK(launch_strack_peak(pk, c->numSM, c->stream), "strack_peak");
+                    c->launches++;
+                }
+            }
         }
         cudaEventRecord(c->sev[1], c->stream);
         FitArgs f = make_fit_args(p, dfit, a.nList, 0, drec);

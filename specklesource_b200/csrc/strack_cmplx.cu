@@ -26,7 +26,7 @@ struct CmplxSmem {
     static constexpr int IMG = W * RS;  // float2 per buffer; three buffers X, Y, Z
     static constexpr int OSD = OSW * NFAST / 2 + 16;  // float2 of the real oversampling table
     static constexpr size_t bytes = sizeof(float2) * (3 * IMG + 2 * W + OSD + NFAST * NFAST + NFAST * OSW) +
-                                    sizeof(float) * (NFAST * NFAST) + sizeof(double) * (NT / 32 + 1) * 8 + 64;
+                                    sizeof(float) * (NFAST * NFAST) + sizeof(double) * (NT / 32 + 1) * 8 + 64 + 16;
 };
 
 // |c|^2 of the 2W x 2W surface at unshifted index (cy, cx).  The parity plane
@@ -301,14 +301,13 @@ __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(Cmp
     float2* T = Yb + NFAST * NFAST;
     float* blk = reinterpret_cast<float*>(T + NFAST * OSW);
     double* red = reinterpret_cast<double*>(blk + NFAST * NFAST);
-    const float* osD = reinterpret_cast<const float*>(osD2);
+    int* azs = reinterpret_cast<int*>(red + (NT / 32 + 1) * 8);  // the patch's roll, set by thread 0
     const int tid = threadIdx.x;
 
     for (int e = tid; e < W; e += NT) {
         twW[e] = a.twW[e];
         tau[e] = a.tau[e];
     }
-    for (int e = tid; e < S::OSD; e += NT) osD2[e] = a.osD[e];
     __syncthreads();
 
     float* smf = reinterpret_cast<float*>(smem_raw);
@@ -354,6 +353,10 @@ __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(Cmp
                 a.rec[p].azset = -1;
                 a.fit[it].point = p;
                 a.fit[it].gate = 0;
+                if constexpr (!GAUSS) {
+                    a.peak[it].point = p;
+                    a.peak[it].iC = PJ_NODATA;
+                }
             }
             continue;  // uniform across the block
         }
@@ -384,7 +387,9 @@ __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(Cmp
             }
         }
         block_allsum<4, NT>(d, red);
-        const int azShift = dop_shift(d[0], d[1], d[2], d[3], W, W);
+        // one thread evaluates the roll (two double atan2); the barriers of the
+        // forward transforms publish it before the row pass reads it
+        if (tid == 0) *azs = dop_shift(d[0], d[1], d[2], d[3], W, W);
         const double p1 = s[0] / n, p2 = s[1] / n;
         // ---------------------------------------------------- baseline flattening
         if (a.baseOn) {
@@ -411,6 +416,7 @@ __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(Cmp
         if (a.intf) phase_correct_int<W, RS, NT>(a, pl, X, Y, red);
         // ---------------------------------------------------- spectra of both patches (X and Z)
         sbfft::fft2d_smem<W, -1, 2, NT, RS, 2 * IMG>(X, twW);
+        const int azShift = *azs;
         // ---------------------------------------------------- padded inverse
         // One dual row pass (over k2) makes R0 (e2 = 0, into Y) and R1 (e2 = 1,
         // times tau[k2], into Z) from the cross spectrum X conj(Z) with the
@@ -456,6 +462,44 @@ __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(Cmp
             iMax = -1000;
             jMax = -1000;
         }
+        if constexpr (!GAUSS) {
+            // ------------------------------------------------ hand the peak to the peak kernel
+            // (overSampleC and the Gaussian-width samples run there, a warp per patch)
+            PeakJob* pj = a.peak + it;
+            constexpr int NB = NFAST * NFAST, NH = 4 * (NGAUSS + 3), NV = (NGAUSS + 3) * 4;
+            if (!rejected) {
+                for (int e = tid; e < NB + NH + NV; e += NT) {
+                    int y, x;
+                    if (e < NB) {
+                        y = iMax - NFAST / 2 + e / NFAST;
+                        x = jMax - NFAST / 2 + e % NFAST;
+                    } else if (e < NB + NH) {
+                        const int q = e - NB;
+                        y = iMax - 2 + q / (NGAUSS + 3);
+                        x = jMax - (NGAUSS / 2 + 2) + q % (NGAUSS + 3);
+                    } else {
+                        const int q = e - NB - NH;
+                        y = iMax - (NGAUSS / 2 + 2) + q / 4;
+                        x = jMax - 2 + q % 4;
+                    }
+                    // blk, hs, vs are consecutive: value e goes to float e of blk
+                    if (y >= 0 && y < W2 && x >= 0 && x < W2) (&pj->blk[0][0])[e] = fmap<W>(smf, y, x);
+                }
+            }
+            if (tid == 0) {
+                pj->point = p;
+                pj->iC = iMax;
+                pj->jC = jMax;
+                pj->p1 = p1;
+                pj->p2 = p2;
+                PointRec* r = &a.rec[p];
+                r->azd = -(float)SB_LARGEINT;  // complexMatch resets aZDefocus (:379)
+                r->azset = azShift;
+                r->flags |= RF_DONE_C | RF_HD_C;
+            }
+            __syncthreads();
+            continue;
+        }
         // samples for gaussPeak1D x 2 through the peak (NOVER units in)
         auto fit_samples = [&](int iMx, int jMx) -> int {
             const int iM = iMx / NOVER, jM = jMx / NOVER;
@@ -473,30 +517,12 @@ __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(Cmp
             }
             return g;
         };
-        int gate = 0;
-        if constexpr (GAUSS) {
-            // cmpTrackGauss on the 2x grid (hanning correction as the oversampling's)
-            const double scale = a.hanCorr / (sqrt(p1 * p2) * pow((double)(W * W), 2));
-            if (!rejected) cMax = (double)sqrtf(fmap<W>(smf, iMax, jMax));
-            gauss2d_peak<NT>([smf](int i, int j) { return sqrtf(fmap<W>(smf, i, j)); }, W2, scale,
-                             reinterpret_cast<float*>(T), blk, iMax, jMax, cMax);
-            gate = fit_samples(iMax, jMax);
-        } else if (!rejected) {
-            // ------------------------------------------------ overSampleC on the 8x8 block
-            if (tid < NFAST * NFAST) {
-                const int t1 = tid / NFAST, t2 = tid % NFAST;
-                blk[tid] = sqrtf(fmap<W>(smf, iMax - NFAST / 2 + t1, jMax - NFAST / 2 + t2));
-            }
-            __syncthreads();
-            const ArgMax ob = oversample_peak_real<NT>(blk, osD, Yb, T, reinterpret_cast<unsigned long long*>(red));
-            const int iMax1 = ob.pos / OSW + (NFAST * NOVER) / 2 - 2 * NOVER;
-            const int jMax1 = ob.pos % OSW + (NFAST * NOVER) / 2 - 2 * NOVER;
-            cMax = (double)ob.v / (NFAST * NFAST);
-            cMax = a.hanCorr * cMax / (sqrt(p1 * p2) * pow((double)(W * W), 2));
-            iMax = (iMax * NOVER) + iMax1 - (NOVER * NFAST) / 2;
-            jMax = (jMax * NOVER) + jMax1 - (NOVER * NFAST) / 2;
-            gate = fit_samples(iMax, jMax);
-        }
+        // cmpTrackGauss on the 2x grid (hanning correction as the oversampling's)
+        const double scale = a.hanCorr / (sqrt(p1 * p2) * pow((double)(W * W), 2));
+        if (!rejected) cMax = (double)sqrtf(fmap<W>(smf, iMax, jMax));
+        gauss2d_peak<NT>([smf](int i, int j) { return sqrtf(fmap<W>(smf, i, j)); }, W2, scale,
+                         reinterpret_cast<float*>(T), blk, iMax, jMax, cMax);
+        const int gate = fit_samples(iMax, jMax);
         if (tid == 0) {
             PointRec* r = &a.rec[p];
             r->cMax[0] = cMax;

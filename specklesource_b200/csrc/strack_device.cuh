@@ -214,6 +214,72 @@ __device__ __forceinline__ unsigned long long am_key(float v, unsigned rank)
 // products with D are real x complex (half the multiplies of A X A^T).
 // osD: D row-major [n][t] (48 x 8 floats, 16-byte aligned) followed by the
 // 16 phases exp(i pi s / 8).  Yb: 64 float2, T: 8 * 48 float2 of scratch.
+// One entry of T = Y D^T: T[t1][n2] = sum_t2 Y[t1][t2] D[n2][t2].
+__device__ __forceinline__ float2 osr_T_entry(const float2* Yb, const float* osD, int t1, int n2)
+{
+    const float4* dr = reinterpret_cast<const float4*>(osD + n2 * NFAST);
+    const float4 d0 = dr[0], d1 = dr[1];
+    const float d[NFAST] = {d0.x, d0.y, d0.z, d0.w, d1.x, d1.y, d1.z, d1.w};
+    float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int t2 = 0; t2 < NFAST; ++t2) {
+        const float2 y = Yb[t1 * NFAST + t2];
+        acc.x = fmaf(d[t2], y.x, acc.x);
+        acc.y = fmaf(d[t2], y.y, acc.y);
+    }
+    return acc;
+}
+
+// Rows n1 = g, g + 8, ..., g + 40 of column n2 of O = D T: the best
+// (|O|, first index) key among them.
+__device__ __forceinline__ unsigned long long osr_O_rows(const float2* T, const float* osD, int g, int n2)
+{
+    constexpr int RPG = OSW / NFAST;
+    float2 tv[NFAST];
+#pragma unroll
+    for (int t1 = 0; t1 < NFAST; ++t1) tv[t1] = T[t1 * OSW + n2];
+    unsigned long long best = 0ull;
+#pragma unroll
+    for (int u = 0; u < RPG; ++u) {
+        const int n1 = g + NFAST * u;
+        const float4* dr = reinterpret_cast<const float4*>(osD + n1 * NFAST);
+        const float4 d0 = dr[0], d1 = dr[1];
+        const float d[NFAST] = {d0.x, d0.y, d0.z, d0.w, d1.x, d1.y, d1.z, d1.w};
+        float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int t1 = 0; t1 < NFAST; ++t1) {
+            acc.x = fmaf(d[t1], tv[t1].x, acc.x);
+            acc.y = fmaf(d[t1], tv[t1].y, acc.y);
+        }
+        const float v = sqrtf(fmaf(acc.x, acc.x, __fmul_rn(acc.y, acc.y)));
+        const unsigned long long k = am_key(v, (unsigned)(n1 * OSW + n2));
+        best = k > best ? k : best;
+    }
+    return best;
+}
+
+__device__ __forceinline__ ArgMax osr_result(unsigned long long best)
+{
+    ArgMax r;
+    if ((best >> 32) == 0ull) {  // nothing above 0: the reference keeps index 0,0
+        r.v = 0.f;
+        r.pos = 0;
+    } else {
+        r.v = __uint_as_float((unsigned)(best >> 32));
+        r.pos = (int)(0xffffffffu - (unsigned)(best & 0xffffffffull));
+    }
+    r.rank = r.pos;
+    return r;
+}
+
+// The same 48 x 48 window through the real form of the matrix:
+//   A[n][t] = p(n) exp(+i pi t / 8) D[n][t],  |p(n)| = 1,
+//   D[n][t] = 2 sum_{g = 1/2, 3/2, 5/2, 7/2} cos(2 pi g (n + 24 - 12 t) / 96),
+// so |O| = |D Y D^T| with Y[t1][t2] = exp(i pi (t1 + t2) / 8) X[t1][t2]; the
+// products with D are real x complex (half the multiplies of A X A^T).
+// osD: D row-major [n][t] (48 x 8 floats, 16-byte aligned) followed by the
+// 16 phases exp(i pi s / 8).  Yb: 64 float2, T: 8 * 48 float2 of scratch.
+// Block version: all NT threads, block barriers.
 template <int NT>
 __device__ __forceinline__ ArgMax oversample_peak_real(const float* blk, const float* osD, float2* Yb, float2* T,
                                                        unsigned long long* scratch)
@@ -226,60 +292,43 @@ __device__ __forceinline__ ArgMax oversample_peak_real(const float* blk, const f
         Yb[tid] = make_float2(x * e.x, x * e.y);
     }
     __syncthreads();
-    // T[t1][n2] = sum_t2 Y[t1][t2] D[n2][t2]
-    for (int e = tid; e < NFAST * OSW; e += NT) {
-        const int t1 = e / OSW, n2 = e % OSW;
-        const float4* dr = reinterpret_cast<const float4*>(osD + n2 * NFAST);
-        const float4 d0 = dr[0], d1 = dr[1];
-        const float d[NFAST] = {d0.x, d0.y, d0.z, d0.w, d1.x, d1.y, d1.z, d1.w};
-        float2 acc = make_float2(0.f, 0.f);
-#pragma unroll
-        for (int t2 = 0; t2 < NFAST; ++t2) {
-            const float2 y = Yb[t1 * NFAST + t2];
-            acc.x = fmaf(d[t2], y.x, acc.x);
-            acc.y = fmaf(d[t2], y.y, acc.y);
-        }
-        T[t1 * OSW + n2] = acc;
-    }
+    for (int e = tid; e < NFAST * OSW; e += NT) T[e] = osr_T_entry(Yb, osD, e / OSW, e % OSW);
     __syncthreads();
-    // O[n1][n2] = sum_t1 D[n1][t1] T[t1][n2]; a thread keeps column n2 of T in
-    // registers and produces rows n1 = g, g + 8, ..., g + 40.
-    constexpr int NG = NFAST;            // row groups
-    constexpr int RPG = OSW / NG;        // rows per thread
+    // a thread keeps column n2 of T in registers and produces rows g, g + 8, ...
     unsigned long long best = 0ull;
-    for (int e = tid; e < NG * OSW; e += NT) {
-        const int n2 = e % OSW, g = e / OSW;
-        float2 tv[NFAST];
-#pragma unroll
-        for (int t1 = 0; t1 < NFAST; ++t1) tv[t1] = T[t1 * OSW + n2];
-#pragma unroll
-        for (int u = 0; u < RPG; ++u) {
-            const int n1 = g + NG * u;
-            const float4* dr = reinterpret_cast<const float4*>(osD + n1 * NFAST);
-            const float4 d0 = dr[0], d1 = dr[1];
-            const float d[NFAST] = {d0.x, d0.y, d0.z, d0.w, d1.x, d1.y, d1.z, d1.w};
-            float2 acc = make_float2(0.f, 0.f);
-#pragma unroll
-            for (int t1 = 0; t1 < NFAST; ++t1) {
-                acc.x = fmaf(d[t1], tv[t1].x, acc.x);
-                acc.y = fmaf(d[t1], tv[t1].y, acc.y);
-            }
-            const float v = sqrtf(acc.x * acc.x + acc.y * acc.y);
-            const unsigned long long k = am_key(v, (unsigned)(n1 * OSW + n2));
-            best = k > best ? k : best;
-        }
+    for (int e = tid; e < NFAST * OSW; e += NT) {
+        const unsigned long long k = osr_O_rows(T, osD, e / OSW, e % OSW);
+        best = k > best ? k : best;
     }
-    best = block_max_u64(best, scratch);
-    ArgMax r;
-    if ((best >> 32) == 0ull) {  // nothing above 0: the reference keeps index 0,0
-        r.v = 0.f;
-        r.pos = 0;
-    } else {
-        r.v = __uint_as_float((unsigned)(best >> 32));
-        r.pos = (int)(0xffffffffu - (unsigned)(best & 0xffffffffull));
+    return osr_result(block_max_u64(best, scratch));
+}
+
+// Warp version (one warp per patch, warp barriers only).  blk: the 8 x 8
+// |c| block (any lane may read it); Yb, T: this warp's scratch.
+__device__ __forceinline__ ArgMax oversample_peak_warp(const float* blk, const float* osD, float2* Yb, float2* T)
+{
+    const int lane = threadIdx.x & 31;
+    const float2* ph = reinterpret_cast<const float2*>(osD + OSW * NFAST);
+    for (int t = lane; t < NFAST * NFAST; t += 32) {
+        const float x = blk[t];
+        const float2 e = ph[t / NFAST + t % NFAST];
+        Yb[t] = make_float2(x * e.x, x * e.y);
     }
-    r.rank = r.pos;
-    return r;
+    __syncwarp();
+    for (int e = lane; e < NFAST * OSW; e += 32) T[e] = osr_T_entry(Yb, osD, e / OSW, e % OSW);
+    __syncwarp();
+    unsigned long long best = 0ull;
+    for (int e = lane; e < NFAST * OSW; e += 32) {
+        const unsigned long long k = osr_O_rows(T, osD, e / OSW, e % OSW);
+        best = k > best ? k : best;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long u = __shfl_xor_sync(0xffffffffu, best, o);
+        best = u > best ? u : best;
+    }
+    __syncwarp();  // Yb and T are free for the next patch
+    return osr_result(best);
 }
 
 // ---------------------------------------------------------------- LM fit

@@ -8,6 +8,34 @@
 
 namespace sbk {
 
+// The neighbourhood of a complex-match peak, handed from the complex kernel
+// to the peak kernel (overSampleC and the gaussPeak1D samples,
+// speckleTrack.c:648-709): |c|^2 of the fftshifted 2W x 2W surface around the
+// coarse peak (iC, jC).  The oversampled peak lies within two samples of it,
+// so the row and column strips hold every sample the two 1-D fits can read.
+struct PeakJob {
+    int32_t point;
+    int32_t iC, jC;       // findCPeak's peak; -1000 when rejected; PJ_NODATA: getPatches failed
+    int32_t pad;
+    double p1, p2;        // patch powers (cMax normalisation)
+    float blk[NFAST][NFAST];        // rows iC-4 .. iC+3, cols jC-4 .. jC+3
+    float hs[4][NGAUSS + 3];        // rows iC-2 .. iC+1, cols jC-11 .. jC+9
+    float vs[NGAUSS + 3][4];        // rows iC-11 .. iC+9, cols jC-2 .. jC+1
+};
+constexpr int32_t PJ_NODATA = -2000000;
+
+// Arguments of the peak kernel (one warp per list position).
+struct PeakArgs {
+    const PeakJob* peak;
+    int nList;
+    int W;                 // complex window (the surface is 2W x 2W)
+    double hanCorr;
+    const float2* osD;     // real oversampling table (48 x 8 floats D, 16 phases)
+    PointRec* rec;
+    FitJob* fit;
+};
+cudaError_t launch_strack_peak(const PeakArgs& a, int numSM, cudaStream_t st);
+
 // Arguments of the complex stage (one grid point per CTA iteration).
 struct CmplxArgs {
     const void* img1;
@@ -38,6 +66,7 @@ struct CmplxArgs {
     int intPs, intPSA, intPSR;  // patch, padded sizes (ps * nal, ps * nrl)
     const float2* twP;          // exp(-2 pi i e / ps), e < ps
     int gauss;                  // -gauss: 2-D Gaussian fit instead of the oversampling
+    PeakJob* peak;              // one entry per list position (unused with -gauss)
 };
 
 // Arguments of an amplitude try (small: s = 1, large: s = LA = 2).

@@ -28,6 +28,9 @@ from . import abi
 # per-point device buffers of one strack call (plan, record, lists, fit job,
 # five output grids), bytes
 _STRACK_POINT_BYTES = 20 + 80 + 16 + 160 + 17 + 64
+# complex-peak hand-off (PeakJob), allocated for at most one list chunk
+_PEAK_JOB_BYTES = 960
+_PEAK_CHUNK = 1 << 19
 # per-CTA workspaces (float2 elements), sized like the kernels' own
 _AMP_SCRATCH = {16: 3 * 16 * 16 + 32 * 32 * 3 // 2, 24: 3 * 24 * 24 + 48 * 48 * 3 // 2,
                 32: 3 * 32 * 32 + 64 * 64 * 3 // 2, 48: 3 * 48 * 48 + 96 * 96 * 3 // 2,
@@ -68,6 +71,8 @@ def job_device_bytes(job, num_sm=148):
     ctas = 2 * num_sm
     if job.kind == "strack":
         b += n * _STRACK_POINT_BYTES
+        if not getattr(p, "gaussFlag", 0):
+            b += min(n, _PEAK_CHUNK) * _PEAK_JOB_BYTES
         if p.maxTries > 0:
             wa = int(p.wRa)
             b += ctas * 8 * _AMP_SCRATCH.get(wa, _AMP_SCRATCH[128])
