@@ -99,7 +99,8 @@ struct MagMax {
 // sqrtf is correctly rounded and monotone, so every position whose sqrtf
 // equals sqrtf(pmax) has |c|^2 within a relative 2^-20 of pmax: only those
 // are ranked.  Returns the fftshifted (iMax, jMax), or (0, 0) when nothing is
-// above 0.  iscr: NT/32 words.
+// above 0.  iscr: 2 NT/32 words, one set per reduction; the caller puts a
+// block barrier between this and the next write to them.
 template <int W, int NT>
 __device__ __forceinline__ void cpeak_from_planes(const float* smf, float pmax, unsigned* iscr, int& iMax, int& jMax)
 {
@@ -110,7 +111,6 @@ __device__ __forceinline__ void cpeak_from_planes(const float* smf, float pmax, 
     u = iscr[0];
 #pragma unroll
     for (int w = 1; w < NT / 32; ++w) u = max(u, iscr[w]);
-    __syncthreads();
     const float pm = __uint_as_float(u);
     iMax = 0;
     jMax = 0;
@@ -134,12 +134,11 @@ __device__ __forceinline__ void cpeak_from_planes(const float* smf, float pmax, 
         }
     }
     best = __reduce_min_sync(0xffffffffu, best);
-    if (lane == 0) iscr[warp] = best;
+    if (lane == 0) iscr[NT / 32 + warp] = best;
     __syncthreads();
-    best = iscr[0];
+    best = iscr[NT / 32];
 #pragma unroll
-    for (int w = 1; w < NT / 32; ++w) best = min(best, iscr[w]);
-    __syncthreads();
+    for (int w = 1; w < NT / 32; ++w) best = min(best, iscr[NT / 32 + w]);
     const int q = best & 3, ij = best >> 2;
     iMax = ij / W + ((q == 1 || q == 2) ? W : 0);
     jMax = ij % W + ((q == 1 || q == 3) ? W : 0);
