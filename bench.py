@@ -819,7 +819,7 @@ def main():
                 "traffic_source": f"ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, profiles/{key}.md"
                                   if traffic else "no committed capture for this workload",
                 "alg_bytes_per_launch": img_bytes + n_pts * (4 * 4 + 1),
-                "kernel": "strack_cmplx_kernel<64,512>",
+                "kernel": "strack_cmplx_kernel<64,256>",
                 "alg_flops_per_patch": ALG_CMPLX,
                 "peak_source": "cuBLAS SGEMM 8192^3 (TF32 off) measured in this run",
                 "hbm": {"achieved_gbs": (img_bytes) / (cm_ms * 1e-3) / 1e9, "peak_gbs": peaks.get("hbm_gbs"),

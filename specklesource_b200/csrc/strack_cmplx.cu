@@ -287,8 +287,8 @@ __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(Cmp
     constexpr int RS = S::RS, IMG = S::IMG;
     constexpr int W2 = 2 * W;
     constexpr int N1 = sbfft::Split<W>::N1, N2 = sbfft::Split<W>::N2;
-    static_assert(NT == 8 * W, "eight threads per column");
-    constexpr int RPT = W / 8;  // consecutive rows per thread in the load phase
+    static_assert((W * W) % NT == 0 && NT % W == 0, "whole rows per thread");
+    constexpr int RPT = W * W / NT;  // consecutive rows per thread in the load phase
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2* X = reinterpret_cast<float2*>(smem_raw);
     float2* Y = X + IMG;
@@ -577,7 +577,7 @@ int cmplx_blocks_per_sm(int W)
     case 24: return occupancy_cmplx<24, 192>();
     case 32: return occupancy_cmplx<32, 256>();
     case 48: return occupancy_cmplx<48, 384>();
-    case 64: return occupancy_cmplx<64, 512>();
+    case 64: return occupancy_cmplx<64, 256>();
     default: return 0;
     }
 }
@@ -589,7 +589,7 @@ cudaError_t launch_strack_cmplx(int W, const CmplxArgs& a, int nCta, cudaStream_
     case 24: return launch_cmplx<24, 192>(a, nCta, st);
     case 32: return launch_cmplx<32, 256>(a, nCta, st);
     case 48: return launch_cmplx<48, 384>(a, nCta, st);
-    case 64: return launch_cmplx<64, 512>(a, nCta, st);
+    case 64: return launch_cmplx<64, 256>(a, nCta, st);
     default: return cudaErrorInvalidValue;
     }
 }
