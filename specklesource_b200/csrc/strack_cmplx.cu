@@ -573,10 +573,10 @@ bool cmplx_supported(int W) { return W == 16 || W == 24 || W == 32 || W == 48 ||
 int cmplx_blocks_per_sm(int W)
 {
     switch (W) {
-    case 16: return occupancy_cmplx<16, 128>();
-    case 24: return occupancy_cmplx<24, 192>();
+    case 16: return occupancy_cmplx<16, 64>();
+    case 24: return occupancy_cmplx<24, 96>();
     case 32: return occupancy_cmplx<32, 256>();
-    case 48: return occupancy_cmplx<48, 384>();
+    case 48: return occupancy_cmplx<48, 192>();
     case 64: return occupancy_cmplx<64, 256>();
     default: return 0;
     }
@@ -585,10 +585,10 @@ int cmplx_blocks_per_sm(int W)
 cudaError_t launch_strack_cmplx(int W, const CmplxArgs& a, int nCta, cudaStream_t st)
 {
     switch (W) {
-    case 16: return launch_cmplx<16, 128>(a, nCta, st);
-    case 24: return launch_cmplx<24, 192>(a, nCta, st);
+    case 16: return launch_cmplx<16, 64>(a, nCta, st);
+    case 24: return launch_cmplx<24, 96>(a, nCta, st);
     case 32: return launch_cmplx<32, 256>(a, nCta, st);
-    case 48: return launch_cmplx<48, 384>(a, nCta, st);
+    case 48: return launch_cmplx<48, 192>(a, nCta, st);
     case 64: return launch_cmplx<64, 256>(a, nCta, st);
     default: return cudaErrorInvalidValue;
     }
