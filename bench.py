@@ -66,6 +66,11 @@ ALG_AMP_L = 2 * _alg_flops_fft(4 * W * W) + 5 * _alg_flops_fft(16 * W * W) + _al
     + _alg_flops_fft(96 * 96)
 
 
+# the library runs the complex stage in list chunks of this many patches
+# (one complex + one peak launch each)
+PEAK_CHUNK = 1 << 19
+
+
 def track_params():
     from specklesource_b200 import abi
     return abi.TrackParams(nR=N_R, nA=N_A, **GRID)
@@ -155,14 +160,14 @@ def fp32_peak_tflops(torch):
 # ---------------------------------------------------------------- CPU baseline
 
 def _cpu_worker(args):
-    band1, band2, aStart, nA, precision = args
+    band1, band2, aStart, nA, nR, precision = args
     sys.path.insert(0, ROOT)
     from oracle import oracle
     from specklesource_b200 import abi
-    p = abi.TrackParams(nR=N_R, nA=nA, **dict(GRID, aStart=aStart))
+    p = abi.TrackParams(nR=nR, nA=nA, **dict(GRID, aStart=aStart))
     t = time.time()
     o = oracle.strack(p, band1, band2, precision=precision)
-    return time.time() - t, nA * N_R, {k: o[k] for k in ("offR", "offA", "type")}
+    return time.time() - t, nA * nR, {k: o[k] for k in ("offR", "offA", "type")}
 
 
 def _row_jobs(img1, img2, rows_per_worker, workers, precision):
@@ -178,8 +183,9 @@ def _row_jobs(img1, img2, rows_per_worker, workers, precision):
         lo = max(0, a_lo)
         b1 = np.ascontiguousarray(img1[lo:a_hi])
         b2 = np.ascontiguousarray(img2[lo:a_hi])
-        # aStart relative to the band keeps the window coordinates of the full grid
-        jobs.append((b1, b2, GRID["aStart"] + i0 * GRID["deltaA"] - lo, rows_per_worker, precision))
+        # aStart relative to the band keeps the window coordinates of the full grid;
+        # the grid width travels with the job (spawned workers see the default workload)
+        jobs.append((b1, b2, GRID["aStart"] + i0 * GRID["deltaA"] - lo, rows_per_worker, N_R, precision))
         starts.append(i0)
     return jobs, starts
 
@@ -805,7 +811,7 @@ def main():
             "dtype": "f32", "data": "synthetic (seeded speckle pair, no public dataset)",
             "config": {"workload": f"strack {NA}x{NR} w64 step 24x6 ({n_pts:,} patches, complex + amplitude "
                                    "fallback)", "parallelism": f"replicas x{world}",
-                       "l2": "inputs 4.6 GB >> 126 MB L2, no flush"},
+                       "l2": f"inputs {img_bytes / 1e9:.2f} GB > 126 MB L2, no flush"},
             "e2e": e2e,
             "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
                            "what": "one sb_strack call over the whole grid, images resident"},
@@ -818,7 +824,9 @@ def main():
                 "traffic": traffic,
                 "traffic_source": f"ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, profiles/{key}.md"
                                   if traffic else "no committed capture for this workload",
-                "alg_bytes_per_launch": img_bytes + n_pts * (4 * 4 + 1),
+                "launch_patches": min(n_pts, PEAK_CHUNK),
+                "launches_per_call": -(-n_pts // PEAK_CHUNK),
+                "alg_bytes_per_launch": int((img_bytes + n_pts * (4 * 4 + 1)) * min(n_pts, PEAK_CHUNK) / n_pts),
                 "kernel": "strack_cmplx_kernel<64,256>",
                 "alg_flops_per_patch": ALG_CMPLX,
                 "peak_source": "cuBLAS SGEMM 8192^3 (TF32 off) measured in this run",
