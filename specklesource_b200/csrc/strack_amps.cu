@@ -388,7 +388,7 @@ bool amps_supported(int Ws) { return Ws == 16 || Ws == 24 || Ws == 32; }
 int amps_blocks_per_sm(int Ws)
 {
     switch (Ws) {
-    case 16: return occupancy_amps<16, 128>();
+    case 16: return occupancy_amps<16, 64>();
     case 24: return occupancy_amps<24, 192>();
     case 32: return occupancy_amps<32, 256>();
     default: return 0;
@@ -398,7 +398,7 @@ int amps_blocks_per_sm(int Ws)
 cudaError_t launch_strack_amps(int Ws, const AmpArgs& a, int nCta, cudaStream_t st)
 {
     switch (Ws) {
-    case 16: return launch_amps<16, 128>(a, nCta, st);
+    case 16: return launch_amps<16, 64>(a, nCta, st);
     case 24: return launch_amps<24, 192>(a, nCta, st);
     case 32: return launch_amps<32, 256>(a, nCta, st);
     default: return cudaErrorInvalidValue;

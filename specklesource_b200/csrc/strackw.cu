@@ -109,7 +109,7 @@ __device__ __forceinline__ float2 sw_sample(const void* img, int nr, int na, int
 template <int W>
 struct SwCfg {
     static constexpr int N = 2 * W;
-    static constexpr int NT = 256;
+    static constexpr int NT = W >= 96 ? 384 : 256;  // 12 warps x 80 registers beat 8 x 128 from W = 96 up
     static constexpr int TILE = sbfft::StagedTile<N, true>::elems > sbfft::StagedTile<W, true>::elems
                                     ? sbfft::StagedTile<N, true>::elems
                                     : sbfft::StagedTile<W, true>::elems;
