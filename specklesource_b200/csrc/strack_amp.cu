@@ -25,7 +25,7 @@ namespace sbk {
 template <int WS>
 struct AmpCfg {
     static constexpr int N = 2 * WS;
-    static constexpr int NT = 256;
+    static constexpr int NT = WS == 64 ? 384 : 256;  // 12 warps x 80 registers win at 64 only (781 vs 868 ms)
     static constexpr int TILE = sbfft::StagedTile<N, true>::elems > sbfft::StagedTile<WS, true>::elems
                                     ? sbfft::StagedTile<N, true>::elems
                                     : sbfft::StagedTile<WS, true>::elems;  // tile and the out-of-place tileB
