@@ -66,6 +66,27 @@ ALG_AMP_L = 2 * _alg_flops_fft(4 * W * W) + 5 * _alg_flops_fft(16 * W * W) + _al
     + _alg_flops_fft(96 * 96)
 
 
+def replica_seed(rank):
+    """Seed of the synthetic pair rank `rank` tracks (each replica its own pair)."""
+    return 2 + 7 * rank
+
+
+def max_over_ranks(torch, value, world, device):
+    """The slowest rank's value: all-reduce MAX over the process group (the
+    job's time is set by its slowest replica).  world <= 1: value itself."""
+    if world <= 1:
+        return value
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world, n_units, ms):
+    """Whole-job units/s of a replica run: every rank processed n_units, the
+    slowest in ms milliseconds."""
+    return world * n_units / (ms * 1e-3)
+
+
 # the library runs the complex stage in list chunks of this many patches
 # (one complex + one peak launch each)
 PEAK_CHUNK = 1 << 19
@@ -729,7 +750,7 @@ def main():
 
     ctx = runtime.Context(local)
     p = track_params()
-    s1, s2 = synth.large_pair(device="cuda", na=NA, nr=NR, seed=2 + 7 * rank)
+    s1, s2 = synth.large_pair(device="cuda", na=NA, nr=NR, seed=replica_seed(rank))
     torch.cuda.synchronize()
     out = {k: torch.empty((N_A, N_R), dtype=torch.float32, device="cuda") for k in ("offR", "offA", "corr", "azd")}
     out["type"] = torch.empty((N_A, N_R), dtype=torch.uint8, device="cuda")
@@ -759,12 +780,8 @@ def main():
     barrier()
     clk = clocks.stop()
     n_pts = N_A * N_R
-    ms_step = tot_ms / args.steps
-    if world > 1:
-        tt = torch.tensor([ms_step], device="cuda")
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        ms_step = float(tt.item())
-    value = world * n_pts / (ms_step * 1e-3)
+    ms_step = max_over_ranks(torch, tot_ms / args.steps, world, "cuda")
+    value = job_rate(world, n_pts, ms_step)
 
     # ---- roofline of the dominant kernel (complex stage, FP32 CUDA cores)
     st0 = stages[-1]
@@ -790,12 +807,8 @@ def main():
             ctx.strack(p, h1, h2, out=hout)
             e_ms += ctx.timing()["total"]
         barrier()
-        e_ms /= args.steps
-        if world > 1:
-            tt = torch.tensor([e_ms], device="cuda")
-            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-            e_ms = float(tt.item())
-        e2e = {"value": world * n_pts / (e_ms * 1e-3), "unit": "patches/s", "h2d_bytes_per_step": img_bytes,
+        e_ms = max_over_ranks(torch, e_ms / args.steps, world, "cuda")
+        e2e = {"value": job_rate(world, n_pts, e_ms), "unit": "patches/s", "h2d_bytes_per_step": img_bytes,
                "d2h_bytes_per_step": n_pts * (4 * 4 + 1), "ms_per_step": e_ms,
                "match_fraction": float((hout["type"] > 0).mean())}
 
