@@ -4,8 +4,8 @@
 // Follows getPatches (Strack/speckleTrack.c:1194-1330), estDopCarrier1
 // (Strack/dopplerEstimation.c:25-88), phaseCorrectBaseline (:868-907),
 // cmpPSWithPad (:604-643), cmpTrackFast (:648-709), findCPeak (:744-805),
-// overSampleC (:852-863), gaussPeak1D (:2137-2202), complexMatch (:349-394)
-// and finalizeCmpxMatch (:714-739).
+// cmpTrackGauss (:2205-2303), gaussPeak1D's samples (:2137-2202),
+// complexMatch (:349-394) and finalizeCmpxMatch (:714-739).
 //
 // The 2W x 2W inverse transform of the zero-padded cross spectrum is computed
 // as four W x W inverse transforms, one per output parity (e1, e2): with the
@@ -13,6 +13,12 @@
 //   c[2 m1 + e1][2 m2 + e2] = IDFT_W(X' tau_e1[k1'] tau_e2[k2'])[m1][m2],
 //   tau_0 = 1, tau_1[k'] = +-exp(+2 pi i k' / 2W) (minus for k' >= W/2),
 // which is the same sum regrouped.  Only |c| is kept (four W x W float planes).
+//
+// After findCPeak the kernel hands the coarse peak and the |c|^2 samples
+// around it to strack_peak.cu (overSampleC and the gaussPeak1D samples, a warp
+// per patch); with -gauss (GAUSS) the 2-D fit runs here instead.  Thread
+// counts per window are set where the kernel is launched (4W threads, 8W at
+// W = 32), measured per window.
 #include <cuda_runtime.h>
 
 #include "strack_device.cuh"
