@@ -121,3 +121,15 @@ def test_same_result_alone_and_in_the_mix():
             assert np.array_equal(a["track"][k], m["track"][k], equal_nan=True), k
         for k in ("offRS", "offAS", "type"):
             assert np.array_equal(a["cull"][k], m["cull"][k], equal_nan=True), k
+
+
+def test_estimate_counts_the_peak_hand_off_once_per_chunk():
+    """The complex stage's 960-byte peak hand-off is held for at most one list
+    chunk (524,288 points); -gauss keeps the fit in the complex kernel."""
+    small = serve.job_device_bytes(_job(100, 100))
+    big = serve.job_device_bytes(_job(2000, 1000))
+    gauss = _job(2000, 1000)
+    gauss.params.gaussFlag = 1
+    per_point = serve._STRACK_POINT_BYTES
+    assert small - 100 * 100 * per_point >= 100 * 100 * 960
+    assert big - serve.job_device_bytes(gauss) == (1 << 19) * 960
