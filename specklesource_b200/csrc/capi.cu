@@ -399,7 +399,7 @@ static int upload_banded(sb_context* c, const sb_image* im[2], const void* dptr[
         const size_t elem = im[i]->sampleType == SB_CFLOAT32 ? 8 : 4;
         if (!im[i]->onDevice) hostBytes += (size_t)im[i]->nr * (size_t)im[i]->na * elem;
     }
-    // about 8 MB per band and image, at most SB_MAX_BANDS bands
+    // about 8 MB per band and image, at most SB_MAX_BANDS bands (matching waits for the first)
     size_t nb = hostBytes / ((size_t)16 << 20);
     b->nb = nb < 1 ? 1 : (nb > (size_t)SB_MAX_BANDS ? SB_MAX_BANDS : (int)nb);
     cudaError_t e;

@@ -13,7 +13,7 @@ struct DevBuf {
     size_t bytes = 0;
 };
 
-constexpr int SB_MAX_BANDS = 16;  // equals sbk::SB_BANDS_MAX
+constexpr int SB_MAX_BANDS = 32;  // equals sbk::SB_BANDS_MAX
 
 struct sb_context {
     int device = 0;

@@ -14,7 +14,7 @@
 namespace sbk {
 
 constexpr int PART_TILE = 1024;  // items per tile (one per thread)
-constexpr int PART_KMAX = 16;    // largest number of keys
+constexpr int PART_KMAX = 32;    // largest number of keys (one warp of part_write_kernel per key)
 
 // ints of device scratch launch_partition needs for n items and K keys
 size_t partition_scratch_ints(int n, int K);

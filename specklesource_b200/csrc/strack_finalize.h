@@ -23,7 +23,7 @@ cudaError_t launch_rec_init(PointRec* rec, int n, cudaStream_t st);
 
 // Band of every complex-list entry for the overlapped upload (at most
 // SB_BANDS_MAX bands): the key of the ordered partition by band.
-constexpr int SB_BANDS_MAX = 16;
+constexpr int SB_BANDS_MAX = 32;
 cudaError_t launch_band_key(const PointPlan* plan, const int* list, int n, int W, int rows1, int rows2, int nb,
                             int* bandOf, cudaStream_t st);
 // key[p] = 0 for the points whose next missing try is `stage`, else -1.
