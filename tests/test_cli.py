@@ -110,6 +110,29 @@ def test_strack_cli_matches_library(tools, tmp_path, pair):
 
 
 @pytest.mark.gpu
+def test_strack_cli_flags_reach_the_library(tools, tmp_path, pair):
+    """-gauss, -noComplex with -singleAmp, -noHanning and -checkAzFocus set the
+    same parameters as the reference's flags (strack.c readArgs): the tool's
+    files equal the library's results for those parameters."""
+    from specklesource_b200 import runtime
+    a, b = pair
+    kv = _setup_track(tmp_path, a, b)
+    base = dict(rStart=40, aStart=40, deltaR=16, deltaA=8, nR=27, nA=25, wR=32, wA=32, wRa=32, wAa=32)
+    cases = [(["-gauss"], dict(gaussFlag=1)),
+             (["-noComplex", "-singleAmp"], dict(noComplex=1, maxTries=1)),
+             (["-noHanning", "-checkAzFocus"], dict(hanningFlag=0, checkAzFocus=1))]
+    with runtime.Context(0) as ctx:
+        for flags, kw in cases:
+            r = _run(tools["strack"], flags + ["track.par"], tmp_path)
+            assert r.returncode == 0, r.stderr
+            out = files.read_track_outputs(str(tmp_path / "out"), kv["nR"], kv["nA"])
+            g = ctx.strack(abi.TrackParams(**base, **kw), a, b)
+            for k, q in (("dr", "offR"), ("da", "offA"), ("cc", "corr"), ("mt", "type")):
+                assert np.array_equal(out[k], g[q]), (flags, k)
+            assert (g["type"] > 0).mean() > 0.9, flags
+
+
+@pytest.mark.gpu
 def test_strackw_and_cullst_cli(tools, tmp_path, pair):
     from specklesource_b200 import runtime
     a, b = pair
