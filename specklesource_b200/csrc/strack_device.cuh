@@ -230,15 +230,19 @@ __device__ __forceinline__ float2 osr_T_entry(const float2* Yb, const float* osD
     return acc;
 }
 
-// Rows n1 = g, g + 8, ..., g + 40 of column n2 of O = D T: the best
-// (|O|, first index) key among them.
-__device__ __forceinline__ unsigned long long osr_O_rows(const float2* T, const float* osD, int g, int n2)
+// Rows n1 = g, g + 8, ..., g + 40 of column n2 of O = D T, folded into the
+// lane's best (|O|, first index) key.  lo is the lane's bound: a value whose
+// |O|^2 lies more than 2^-20 (relative) below the |O|^2 of the lane's best
+// can neither beat nor tie it after the correctly rounded sqrtf, so the sqrt
+// and the key are evaluated only at or above lo (NaN never is, as NaN never
+// won before).  Start with best = 0, lo = 0.
+__device__ __forceinline__ void osr_O_rows(const float2* T, const float* osD, int g, int n2, unsigned long long& best,
+                                           float& lo)
 {
     constexpr int RPG = OSW / NFAST;
     float2 tv[NFAST];
 #pragma unroll
     for (int t1 = 0; t1 < NFAST; ++t1) tv[t1] = T[t1 * OSW + n2];
-    unsigned long long best = 0ull;
 #pragma unroll
     for (int u = 0; u < RPG; ++u) {
         const int n1 = g + NFAST * u;
@@ -251,11 +255,15 @@ __device__ __forceinline__ unsigned long long osr_O_rows(const float2* T, const 
             acc.x = fmaf(d[t1], tv[t1].x, acc.x);
             acc.y = fmaf(d[t1], tv[t1].y, acc.y);
         }
-        const float v = sqrtf(fmaf(acc.x, acc.x, __fmul_rn(acc.y, acc.y)));
-        const unsigned long long k = am_key(v, (unsigned)(n1 * OSW + n2));
-        best = k > best ? k : best;
+        const float m2 = fmaf(acc.x, acc.x, __fmul_rn(acc.y, acc.y));
+        if (m2 >= lo) {
+            const unsigned long long k = am_key(sqrtf(m2), (unsigned)(n1 * OSW + n2));
+            if (k > best) {
+                best = k;
+                lo = m2 * (1.0f - 1.0f / 1048576.0f);
+            }
+        }
     }
-    return best;
 }
 
 __device__ __forceinline__ ArgMax osr_result(unsigned long long best)
@@ -296,10 +304,8 @@ __device__ __forceinline__ ArgMax oversample_peak_real(const float* blk, const f
     __syncthreads();
     // a thread keeps column n2 of T in registers and produces rows g, g + 8, ...
     unsigned long long best = 0ull;
-    for (int e = tid; e < NFAST * OSW; e += NT) {
-        const unsigned long long k = osr_O_rows(T, osD, e / OSW, e % OSW);
-        best = k > best ? k : best;
-    }
+    float lo = 0.f;
+    for (int e = tid; e < NFAST * OSW; e += NT) osr_O_rows(T, osD, e / OSW, e % OSW, best, lo);
     return osr_result(block_max_u64(best, scratch));
 }
 
@@ -318,10 +324,8 @@ __device__ __forceinline__ ArgMax oversample_peak_warp(const float* blk, const f
     for (int e = lane; e < NFAST * OSW; e += 32) T[e] = osr_T_entry(Yb, osD, e / OSW, e % OSW);
     __syncwarp();
     unsigned long long best = 0ull;
-    for (int e = lane; e < NFAST * OSW; e += 32) {
-        const unsigned long long k = osr_O_rows(T, osD, e / OSW, e % OSW);
-        best = k > best ? k : best;
-    }
+    float lo = 0.f;
+    for (int e = lane; e < NFAST * OSW; e += 32) osr_O_rows(T, osD, e / OSW, e % OSW, best, lo);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         const unsigned long long u = __shfl_xor_sync(0xffffffffu, best, o);
