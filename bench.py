@@ -88,7 +88,7 @@ def job_rate(world, n_units, ms):
 
 
 # the library runs the complex stage in list chunks of this many patches
-# (one complex + one peak launch each)
+# (one complex + one peak launch each; kPeakChunk in csrc/capi.cu)
 PEAK_CHUNK = 1 << 19
 
 

@@ -689,7 +689,7 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
         // peak hand-off buffer: list chunks of at most kPeakChunk patches, each
         // launched as complex kernel + peak kernel (-gauss keeps the fit in
         // the complex kernel)
-        constexpr int kPeakChunk = 1 << 19;
+        constexpr int kPeakChunk = 1 << 19;  // bench.py and serve.py's memory estimate use the same figure
         PeakJob* dpeak = nullptr;
         if (!p->gaussFlag) {
             const size_t pc = nC < kPeakChunk ? (size_t)nC : (size_t)kPeakChunk;

@@ -28,7 +28,8 @@ from . import abi
 # per-point device buffers of one strack call (plan, record, lists, fit job,
 # five output grids), bytes
 _STRACK_POINT_BYTES = 20 + 80 + 16 + 160 + 17 + 64
-# complex-peak hand-off (PeakJob), allocated for at most one list chunk
+# complex-peak hand-off (PeakJob, csrc/strack_kernels.h), allocated for at
+# most one list chunk (kPeakChunk in csrc/capi.cu)
 _PEAK_JOB_BYTES = 960
 _PEAK_CHUNK = 1 << 19
 # per-CTA workspaces (float2 elements), sized like the kernels' own
