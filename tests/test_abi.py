@@ -90,3 +90,23 @@ def test_ctypes_layout_matches_header(tmp_path):
         assert got[(cname, "size")] == C.sizeof(cls), cname
         for fname, _ in cls._fields_:
             assert got[(cname, fname)] == getattr(cls, fname).offset, (cname, fname)
+
+
+def test_peak_hand_off_constants_agree(tmp_path):
+    """The complex stage's list chunk and PeakJob size, as the library defines
+    them, are the figures bench.py and the job server's memory estimate use."""
+    import re
+
+    import bench
+    from specklesource_b200 import serve
+    src = open(os.path.join(ROOT, "specklesource_b200", "csrc", "capi.cu")).read()
+    chunk = 1 << int(re.search(r"kPeakChunk = 1 << (\d+);", src).group(1))
+    assert chunk == bench.PEAK_CHUNK == serve._PEAK_CHUNK
+    prog = tmp_path / "pj.cu"
+    prog.write_text('#include <cstdio>\n#include "strack_kernels.h"\n'
+                    'int main() { std::printf("%zu\\n", sizeof(sbk::PeakJob)); return 0; }\n')
+    exe = tmp_path / "pj"
+    subprocess.run(["nvcc", "-std=c++17", "-I", os.path.join(ROOT, "specklesource_b200", "csrc"), str(prog), "-o",
+                    str(exe)], check=True, capture_output=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout
+    assert int(out) == serve._PEAK_JOB_BYTES
