@@ -7,6 +7,10 @@
  * FFTW 2.1.5 itself is not in the reference tree; this is an independent
  * implementation of the same mathematical transform, written from the DFT
  * definition (recursive decimation in time over the prime factors of N).
+ * Built with OFFT_BATCHED (the float library, the timed CPU baseline), the 2-D
+ * transform is instead a self-sorting (Stockham) decimation-in-frequency FFT
+ * applied to whole rows at a time, which a compiler vectorises: FFTW is an
+ * optimised library, so the baseline's FFT has to be a competitive one.
  */
 #ifndef ORACLE_FFT_REF_H
 #define ORACLE_FFT_REF_H
@@ -30,11 +34,17 @@ void offt_destroy(offt_plan *p);
 /* out-of-place 1-D transform; in and out must not overlap */
 void offt_exec_1d(const offt_plan *p, const ocplx *in, ocplx *out);
 
+typedef struct offt_batch offt_batch;
+
 typedef struct {
     int na, nr;
     offt_plan *rows; /* length nr */
     offt_plan *cols; /* length na */
     ocplx *tmpA, *tmpB;
+    /* OFFT_BATCHED builds: self-sorting transforms batched across the other
+     * axis (see fft_ref.c), with three na x nr work arrays */
+    offt_batch *brows, *bcols;
+    ocplx *w0, *w1, *w2;
 } offt2d;
 
 offt2d *offt2d_plan(int na, int nr, int sign);

@@ -51,6 +51,7 @@ int oracle_est_dop_carrier(const float *p1, const float *p2, int32_t nAz, int32_
 /* 2-D DFT helper exposed for FFT tests: in-place on interleaved REAL data
  * passed as double (converted internally). */
 int oracle_fft2d(double *data, int32_t na, int32_t nr, int32_t sign);
+int oracle_fft2d_time(int32_t na, int32_t nr, int32_t reps, double *secs);
 
 /* sizeof(REAL): 4 or 8 */
 int oracle_real_size(void);

@@ -43,6 +43,8 @@ def lib(precision="f64"):
         L.oracle_est_dop_carrier.restype = C.c_int
         L.oracle_fft2d.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]
         L.oracle_fft2d.restype = C.c_int
+        L.oracle_fft2d_time.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_double)]
+        L.oracle_fft2d_time.restype = C.c_int
         L.oracle_real_size.restype = C.c_int
         _LIBS[precision] = L
     return _LIBS[precision]
@@ -126,6 +128,14 @@ def est_dop_carrier(p1, p2, wA):
     b = np.ascontiguousarray(p2, np.complex64)
     nAz, nRg = a.shape
     return lib("f64").oracle_est_dop_carrier(a.ctypes.data, b.ctypes.data, nAz, nRg, wA)
+
+
+def fft2d_time(na, nr, reps, precision="f32"):
+    """Seconds per forward na x nr transform of the restatement's FFT (plan
+    made once, one thread)."""
+    t = C.c_double(0.0)
+    lib(precision).oracle_fft2d_time(na, nr, reps, C.byref(t))
+    return t.value
 
 
 def fft2d(x, sign=-1, precision="f64"):

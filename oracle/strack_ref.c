@@ -25,6 +25,7 @@
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 
 #include "fft_ref.h"
 #include "oracle.h"
@@ -1255,6 +1256,30 @@ int oracle_est_dop_carrier(const float *p1, const float *p2, int32_t nAz, int32_
     free(a);
     free(b);
     return s;
+}
+
+/* Seconds per forward 2-D transform of na x nr in this build's precision:
+ * the plan is made once, then reps executions are timed (one thread).  Used
+ * to compare the CPU baseline's FFT with another FFT library's. */
+int oracle_fft2d_time(int32_t na, int32_t nr, int32_t reps, double *secs)
+{
+    size_t n = (size_t)na * nr;
+    ocplx *a = cbuf(n), *o = cbuf(n);
+    for (size_t k = 0; k < n; k++) {
+        a[k].re = (REAL)((double)((k * 7919u) % 1000u) / 1000.0 - 0.5);
+        a[k].im = (REAL)((double)((k * 104729u) % 1000u) / 1000.0 - 0.5);
+    }
+    offt2d *pl = offt2d_plan(na, nr, OFFT_FORWARD);
+    offt2d_exec(pl, a, o);
+    struct timespec t0, t1;
+    clock_gettime(CLOCK_MONOTONIC, &t0);
+    for (int32_t r = 0; r < reps; r++) offt2d_exec(pl, a, o);
+    clock_gettime(CLOCK_MONOTONIC, &t1);
+    *secs = ((double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec)) / (reps > 0 ? reps : 1);
+    offt2d_destroy(pl);
+    free(a);
+    free(o);
+    return SB_OK;
 }
 
 int oracle_fft2d(double *data, int32_t na, int32_t nr, int32_t sign)
