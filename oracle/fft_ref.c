@@ -336,17 +336,6 @@ __attribute__((unused)) static ocplx *ob_exec(const offt_batch *b, ocplx *a, ocp
     return x;
 }
 
-__attribute__((unused)) static void ob_transpose(const ocplx *in, ocplx *out, int rows, int cols)
-{
-    const int B = 32;
-    for (int i0 = 0; i0 < rows; i0 += B)
-        for (int j0 = 0; j0 < cols; j0 += B) {
-            const int i1 = i0 + B < rows ? i0 + B : rows, j1 = j0 + B < cols ? j0 + B : cols;
-            for (int i = i0; i < i1; i++)
-                for (int j = j0; j < j1; j++) out[(size_t)j * rows + i] = in[(size_t)i * cols + j];
-        }
-}
-
 offt2d *offt2d_plan(int na, int nr, int sign)
 {
     offt2d *p = (offt2d *)calloc(1, sizeof(offt2d));
