@@ -1,12 +1,17 @@
 /*
- * cull_ref.c -- TEST INFRASTRUCTURE ONLY (CPU oracle, parity unpinned).
+ * cull_ref.c -- TEST INFRASTRUCTURE ONLY (CPU oracle, pinned to the reference build by tests/test_ref_pin.py).
  *
  * Restatement of the cullst pipeline: Cullst/cullst.c:36-121,
  * Cullst/cullSTData.c, cullStats.c, cullSmooth.c, cullIslands.c.  The
  * arithmetic keeps the reference's float/double types (both oracle builds are
  * identical here).  Third-party pieces absent from the reference tree:
- *  - Numerical Recipes select (selectForCull is a copy of it in the tree):
- *    restated as "k-th smallest value, 1-based", which is what it returns.
+ *  - selectForCull (cullSTData.c:132-192, Numerical Recipes' select adapted):
+ *    restated as "k-th smallest value, 1-based", which is what it is written
+ *    to return.  As compiled, it does not: at :160 the three-statement SWAP
+ *    macro follows an unbraced if, so two of its statements always run and
+ *    read an uninitialised temporary; the value it returns then depends on
+ *    the compiler (tests/test_ref_pin.py).  With nGood = 0 a box with one
+ *    valid point makes it return listR[0], which is never written.
  *  - Numerical Recipes svdfit (cullStats.c:91-95): least squares by SVD with
  *    singular values below 1e-5 * max zeroed (the published svdfit TOL);
  *    restated through the eigen-decomposition of the 3x3 normal matrix.

@@ -3,12 +3,14 @@
  * hot path, used by tests/, __graft_entry__.smoke() and bench.py's CPU
  * baseline leg as the checker.  Nothing in the product links it.
  *
- * PARITY UNPINNED: the reference cannot be compiled (it links FFTW 2.1.5,
- * Numerical Recipes, GDAL and GrIMP libraries that are not in its tree) and
- * ships no tests, fixtures or golden vectors.  This restatement is checked
- * against known-answer tests (integer and sub-pixel shifts, empty patches,
- * hand-built cull grids) in tests/test_oracle_kat.py.
- *
+ * Parity pinned to the reference's own code: the reference's hot-path
+ * sources (Strack/speckleTrack.c, Strackw/corrTrackFast.c, Cullst/cull*.c)
+ * compile unmodified against stand-ins for the libraries its tree lacks
+ * (oracle/refshim/; `make ref` -> oracle/_ref/), and tests/test_ref_pin.py
+ * checks this restatement against them (offsets and match types identical)
+ * live and through committed fixtures of their outputs
+ * (tests/golden/ref_small.npz).  Known-answer tests of its own are in
+ * tests/test_oracle_kat.py.
  * Built twice from the same sources:
  *   liboracle_f64.so  REAL=double, FLT=double  -- the FP64 oracle
  *   liboracle_f32.so  REAL=float,  FLT=float   -- reference-like precision,

@@ -1,7 +1,9 @@
 """TEST INFRASTRUCTURE ONLY: ctypes wrapper of the CPU oracle (oracle/lib/*.so).
 
-Parity unpinned: the reference cannot be built and has no golden vectors; the
-oracle is pinned by the known-answer tests in tests/test_oracle_kat.py.
+Pinned to the reference's own code: tests/test_ref_pin.py compares it with the
+reference's hot-path sources compiled against oracle/refshim/ (oracle/refpin.py)
+and with committed outputs of that build; known-answer tests of its own are in
+tests/test_oracle_kat.py.
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this.
 """
 import ctypes as C

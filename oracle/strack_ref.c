@@ -1,5 +1,5 @@
 /*
- * strack_ref.c -- TEST INFRASTRUCTURE ONLY (CPU oracle, parity unpinned).
+ * strack_ref.c -- TEST INFRASTRUCTURE ONLY (CPU oracle, pinned to the reference build by tests/test_ref_pin.py).
  *
  * Restatement of speckleTrack() and its helpers, Strack/speckleTrack.c and
  * Strack/dopplerEstimation.c.  Each function cites the reference lines it

@@ -1,5 +1,5 @@
 /*
- * strackw_ref.c -- TEST INFRASTRUCTURE ONLY (CPU oracle, parity unpinned).
+ * strackw_ref.c -- TEST INFRASTRUCTURE ONLY (CPU oracle, pinned to the reference build by tests/test_ref_pin.py).
  *
  * Restatement of corrTrackFast() and its helpers, Strackw/corrTrackFast.c.
  * REAL = the reference's fftw_real, FLT = its `float` working variables

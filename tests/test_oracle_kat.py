@@ -1,10 +1,10 @@
-"""Known-answer tests that pin the CPU oracle (the reference ships none).
+"""Known-answer tests of the CPU oracle (the reference ships none).
 
-The reference cannot be built here and has no golden vectors, so parity is
-"unpinned"; these tests pin the oracle to properties the reference's
-algorithm must have: FFTW-convention transforms, exact recovery of integer and
-band-limited sub-pixel shifts, in-band failure values, and the cull rules on
-hand-built grids.
+Beside the comparison with the reference's own code (tests/test_ref_pin.py),
+these tests pin the oracle to properties the reference's algorithm must have:
+FFTW-convention transforms, exact recovery of integer and band-limited
+sub-pixel shifts, in-band failure values, and the cull rules on hand-built
+grids.
 """
 import numpy as np
 import pytest
