@@ -16,7 +16,10 @@ e2e   : patches/s through the C ABI with big-endian host images in pinned
 Inputs (4.6 GB) are far larger than L2 (126 MB), so no flush is needed.
 accuracy: the last step's offsets against the FP64 oracle on a spread sample
         of grid rows (one per host core): error percentiles in px, the
-        fraction within 0.02 px (0.01 px for complex matches), match agreement.
+        fraction within 0.02 px (0.01 px for complex matches), match
+        agreement, and the per-peak-value (corr) error percentiles.
+parity_other_configs: the same figures for cfg1 (whole 1024 x 2048 grid,
+        W = 32) and for strackw at the cfg3 geometry (240 points).
 Under torchrun every rank tracks its own pair (weak scaling, no collective on
 the data path); rank 0 prints the max-over-ranks time.
 """
@@ -188,7 +191,7 @@ def _cpu_worker(args):
     p = abi.TrackParams(nR=nR, nA=nA, **dict(GRID, aStart=aStart))
     t = time.time()
     o = oracle.strack(p, band1, band2, precision=precision)
-    return time.time() - t, nA * nR, {k: o[k] for k in ("offR", "offA", "type")}
+    return time.time() - t, nA * nR, {k: o[k] for k in ("offR", "offA", "corr", "type")}
 
 
 def _row_jobs(img1, img2, rows_per_worker, workers, precision):
@@ -255,40 +258,67 @@ def cpu_baseline(img1, img2, rows_per_worker=32, workers=None):
     pts = sum(r[1] for r in res)
     work = max(r[0] for r in res)
     return {"value": pts / work, "unit": "patches/s", "cores": workers, "kind": "port",
+            "sample_patches": pts, "sample_s": work,
             "sample": f"{workers} processes x {rows_per_worker} grid rows x {N_R} patches ({pts} patches) of "
                       f"the same workload spread over the grid, f32 CPU restatement (oracle/, gcc -O3, "
                       f"vectorised 2-D FFT), {work:.1f} s compute, {wall:.1f} s wall incl. spawn",
             "fft_vs_scipy": fft_vs_scipy()}
 
 
-def accuracy_vs_fp64(img1, img2, gpu, rows_per_worker=1, workers=None):
-    """Offsets of the GPU run against the FP64 oracle on a spread sample of grid
-    rows: error percentiles (px) on the points both match, the fraction within
-    0.02 px (0.01 px for complex matches), and match-type agreement."""
-    workers = workers or os.cpu_count()
-    jobs, starts = _row_jobs(img1, img2, rows_per_worker, workers, "f64")
-    res, wall = _run_pool(jobs)
-    errs, tol_ok, n_match, same, n_pts = [], 0, 0, 0, 0
-    for (_, _, o), i0 in zip(res, starts):
-        sl = slice(i0, i0 + rows_per_worker)
-        g = {k: gpu[k][sl] for k in ("offR", "offA", "type")}
+def corr_errors(g_corr, o_corr, both):
+    """Per-peak-value error of the GPU's correlation against the FP64 oracle
+    on the points both match: absolute and relative percentiles."""
+    if not both.any():
+        return {"corr_abs_p50": None, "corr_abs_p99": None, "corr_abs_max": None, "corr_rel_p99": None}
+    d = np.abs(g_corr[both].astype(np.float64) - o_corr[both])
+    r = d / np.maximum(1e-6, np.abs(o_corr[both]))
+    return {"corr_abs_p50": float(np.percentile(d, 50)), "corr_abs_p99": float(np.percentile(d, 99)),
+            "corr_abs_max": float(d.max()), "corr_rel_p50": float(np.percentile(r, 50)),
+            "corr_rel_p99": float(np.percentile(r, 99)), "corr_rel_max": float(r.max())}
+
+
+def _accuracy_blocks(pairs):
+    """Parity figures over (gpu, oracle) grid pieces: offset error percentiles
+    (px) and per-peak-value (corr) error on the points both match, the
+    fraction within 0.02 px (0.01 px for complex matches), match agreement."""
+    errs, gc, oc, ok, n_match, same, n_pts = [], [], [], 0, 0, 0, 0
+    for g, o in pairs:
         matched = o["type"] > 0
         both = matched & (g["type"] > 0)
         e = np.maximum(np.abs(g["offR"].astype(np.float64) - o["offR"]),
                        np.abs(g["offA"].astype(np.float64) - o["offA"]))
         tol = np.where(o["type"] == 1, 0.01, 0.02)
-        tol_ok += int((both & (e <= tol)).sum())
+        ok += int((both & (e <= tol)).sum())
         n_match += int(matched.sum())
         same += int((g["type"] == o["type"]).sum())
         n_pts += o["type"].size
         errs.append(e[both])
+        gc.append(g["corr"][both])
+        oc.append(o["corr"][both])
     e = np.concatenate(errs) if errs else np.zeros(0)
-    return {"points": n_pts, "oracle_matches": n_match,
-            "frac_within_tol": tol_ok / max(1, n_match), "frac_same_type": same / max(1, n_pts),
-            "err_px_p50": float(np.percentile(e, 50)) if e.size else None,
-            "err_px_p99": float(np.percentile(e, 99)) if e.size else None,
-            "err_px_max": float(e.max()) if e.size else None,
-            "sample": f"{workers} x {rows_per_worker} grid rows spread over the grid, FP64 oracle, {wall:.1f} s"}
+    pct = (lambda q: float(np.percentile(e, q)) if e.size else None)
+    gcv = np.concatenate(gc) if gc else np.zeros(0, np.float32)
+    ocv = np.concatenate(oc) if oc else np.zeros(0)
+    out = {"points": n_pts, "oracle_matches": n_match, "frac_within_tol": ok / max(1, n_match),
+           "frac_same_type": same / max(1, n_pts), "err_px_p50": pct(50), "err_px_p99": pct(99),
+           "err_px_max": float(e.max()) if e.size else None}
+    out.update(corr_errors(gcv, ocv, np.ones(gcv.size, bool)))
+    return out
+
+
+def accuracy_vs_fp64(img1, img2, gpu, rows_per_worker=1, workers=None):
+    """Offsets and correlations of the GPU run against the FP64 oracle on a
+    spread sample of grid rows (see _accuracy_blocks)."""
+    workers = workers or os.cpu_count()
+    jobs, starts = _row_jobs(img1, img2, rows_per_worker, workers, "f64")
+    res, wall = _run_pool(jobs)
+    pairs = []
+    for (_, _, o), i0 in zip(res, starts):
+        sl = slice(i0, i0 + rows_per_worker)
+        pairs.append(({k: gpu[k][sl] for k in ("offR", "offA", "corr", "type")}, o))
+    out = _accuracy_blocks(pairs)
+    out["sample"] = f"{workers} x {rows_per_worker} grid rows spread over the grid, FP64 oracle, {wall:.1f} s"
+    return out
 
 
 def measured_traffic(kernel_key):
@@ -305,6 +335,35 @@ def measured_traffic(kernel_key):
     return None
 
 
+def parity_other_configs(ctx):
+    """Parity of the other tracking configurations against the FP64 oracle,
+    recorded on the bench line: cfg1 (strack, 1024 x 2048 pair, W = 32, step
+    16 x 8, the whole 124 x 119 grid, complex + amplitude fallback) and the
+    cfg3 geometry (strackw, search window 224, edge pad 48, navg 2) on 240
+    points spread over a 2000 x 4000 shear-zone pair."""
+    from specklesource_b200 import abi, synth
+    cores = os.cpu_count()
+    out = {}
+    s1, s2 = synth.small_pair(device="cuda", na=1024, nr=2048)
+    a, b = synth.to_numpy(s1), synth.to_numpy(s2)
+    g1 = dict(rStart=40, aStart=40, deltaR=16, deltaA=8, nR=124, nA=119, wR=32, wA=32, wRa=32, wAa=32)
+    res = ctx.strack(abi.TrackParams(**g1), a, b)
+    rows = (g1["nA"] + cores - 1) // cores
+    blocks = [(i0, min(rows, g1["nA"] - i0), 0, g1["nR"]) for i0 in range(0, g1["nA"], rows)]
+    r64, wall = _oracle_bands("strack", a, b, g1, blocks, 2 * 32 + 48, "f64")
+    out["cfg1_strack_1024x2048_w32"] = dict(_accuracy(r64, blocks, res), oracle_s=wall)
+    s1, s2 = synth.shear_pair(device="cuda", na=2000, nr=4000, seed=3)
+    a, b = synth.to_numpy(s1), synth.to_numpy(s2)
+    del s1, s2
+    g3 = dict(rStart=160, aStart=160, deltaR=160, deltaA=140, nR=20, nA=12, wR=224, wA=224, wRa=224, wAa=224,
+              edgePadR=48, edgePadA=48, navgR=2, navgA=2)
+    res = ctx.strackw(abi.TrackParams(**g3), a, b)
+    blocks = [(i, 1, 0, g3["nR"]) for i in range(g3["nA"])]
+    r64, wall = _oracle_bands("strackw", a, b, g3, blocks, 224, "f64")
+    out["cfg3_strackw_2000x4000_shear_w224"] = dict(_accuracy(r64, blocks, res), oracle_s=wall)
+    return out
+
+
 # ---------------------------------------------------------------- main
 
 def pinned_big_endian(torch, t):
@@ -319,7 +378,18 @@ def pinned_big_endian(torch, t):
     return host.numpy().view(">c8").reshape(na, nr)
 
 
+def bench_config(world):
+    """The `config` of the bench line, shared by both arms."""
+    img_bytes = 2 * NA * NR * 8
+    return {"workload": f"strack {NA}x{NR} w64 step 24x6 ({N_A * N_R:,} patches, complex + amplitude fallback)",
+            "parallelism": f"replicas x{world}", "l2": f"inputs {img_bytes / 1e9:.2f} GB > 126 MB L2, no flush"}
+
+
 def run_reference(args):
+    """The reference arm: the CPU restatement of the path on all host cores
+    (the reference itself needs FFTW 2, Numerical Recipes and GDAL, absent
+    here).  Each step tracks a bounded sample of the workload's grid rows;
+    ms_per_step is that sample's measured time, not the whole grid's."""
     import torch
     from specklesource_b200 import synth
     rank = int(os.environ.get("RANK", "0"))
@@ -330,21 +400,26 @@ def run_reference(args):
     a = synth.to_numpy(s1)
     b = synth.to_numpy(s2)
     del s1, s2
-    vals = []
+    vals, secs = [], []
     cb = None
     for k in range(args.warmup + args.steps):
         rows = 1 if k < args.warmup else args.cpu_rows
         r = cpu_baseline(a, b, rows_per_worker=rows)
         if k >= args.warmup:
             vals.append(r["value"])
+            secs.append(r["sample_s"])
             cb = r
     v = float(np.median(vals))
     line = {"impl": "reference", "metric": METRIC, "value": v,
             "unit": "patches/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * N_A * N_R / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic (seeded speckle pair, no public dataset)",
-            "config": {"workload": "strack 12000x24000 w64 step 24x6 (1,955,217 patches)",
-                       "sample": "bounded CPU sample per step"},
+            "ms_per_step": 1e3 * float(np.median(secs)), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded speckle pair, no public dataset)",
+            "config": bench_config(args.gpus),
+            "step": {"what": "one bounded sample of the workload per step: the CPU restatement on "
+                             f"{cb['cores']} processes x {args.cpu_rows} grid rows spread over the grid",
+                     "sample_patches_per_step": cb["sample_patches"],
+                     "ms_per_step_measured_on_sample": True,
+                     "ms_full_grid_extrapolated": 1e3 * N_A * N_R / v},
             "cpu_baseline": dict(cb, value=v),
             "e2e": {"value": v, "unit": "patches/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -366,7 +441,7 @@ def _band_worker(args):
     p = abi.TrackParams(**grid)
     t = time.time()
     o = getattr(oracle, fn)(p, band1, band2, precision=precision)
-    return time.time() - t, grid["nA"] * grid["nR"], {k: o[k] for k in ("offR", "offA", "type")}
+    return time.time() - t, grid["nA"] * grid["nR"], {k: o[k] for k in ("offR", "offA", "corr", "type")}
 
 
 def _oracle_bands(fn, img1, img2, grid, row_blocks, margin, precision):
@@ -389,24 +464,10 @@ def _oracle_bands(fn, img1, img2, grid, row_blocks, margin, precision):
 
 
 def _accuracy(res, blocks, gpu):
-    errs, ok, n_match, same, n_pts = [], 0, 0, 0, 0
+    pairs = []
     for (_, _, o), (i0, nrows, j0, ncols) in zip(res, blocks):
-        g = {k: gpu[k][i0:i0 + nrows, j0:j0 + ncols] for k in ("offR", "offA", "type")}
-        matched = o["type"] > 0
-        both = matched & (g["type"] > 0)
-        e = np.maximum(np.abs(g["offR"].astype(np.float64) - o["offR"]),
-                       np.abs(g["offA"].astype(np.float64) - o["offA"]))
-        tol = np.where(o["type"] == 1, 0.01, 0.02)
-        ok += int((both & (e <= tol)).sum())
-        n_match += int(matched.sum())
-        same += int((g["type"] == o["type"]).sum())
-        n_pts += o["type"].size
-        errs.append(e[both])
-    e = np.concatenate(errs) if errs else np.zeros(0)
-    pct = (lambda q: float(np.percentile(e, q)) if e.size else None)
-    return {"points": n_pts, "oracle_matches": n_match, "frac_within_tol": ok / max(1, n_match),
-            "frac_same_type": same / max(1, n_pts), "err_px_p50": pct(50), "err_px_p99": pct(99),
-            "err_px_max": float(e.max()) if e.size else None}
+        pairs.append(({k: gpu[k][i0:i0 + nrows, j0:j0 + ncols] for k in ("offR", "offA", "corr", "type")}, o))
+    return _accuracy_blocks(pairs)
 
 
 def _time_calls(ctx, call, steps, warmup):
@@ -838,15 +899,17 @@ def main():
                "d2h_bytes_per_step": n_pts * (4 * 4 + 1), "ms_per_step": e_ms,
                "match_fraction": float((hout["type"] > 0).mean())}
 
-    cpu, acc = None, None
+    cpu, acc, parity = None, None, None
     if rank == 0 and world == 1 and not (args.no_cpu_baseline and args.no_accuracy):
         a = synth.to_numpy(s1)
         b = synth.to_numpy(s2)
         if not args.no_cpu_baseline:
             cpu = cpu_baseline(a, b, rows_per_worker=args.cpu_rows)
         if not args.no_accuracy:
-            g = {k: out[k].cpu().numpy() for k in ("offR", "offA", "type")}
+            g = {k: out[k].cpu().numpy() for k in ("offR", "offA", "corr", "type")}
             acc = accuracy_vs_fp64(a, b, g)
+            del a, b
+            parity = parity_other_configs(ctx)
     key = f"strack_cmplx_w64_{NA}x{NR}"
     traffic = measured_traffic(key)
 
@@ -856,13 +919,12 @@ def main():
             "value": value, "unit": "patches/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded speckle pair, no public dataset)",
-            "config": {"workload": f"strack {NA}x{NR} w64 step 24x6 ({n_pts:,} patches, complex + amplitude "
-                                   "fallback)", "parallelism": f"replicas x{world}",
-                       "l2": f"inputs {img_bytes / 1e9:.2f} GB > 126 MB L2, no flush"},
+            "config": bench_config(world),
             "e2e": e2e,
             "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
                            "what": "one sb_strack call over the whole grid, images resident"},
             "accuracy": acc,
+            "parity_other_configs": parity,
             "gpu_launches": launches,
             "stages": {k: float(np.mean([s[k] for s in stages])) for k in stages[-1]},
             "roofline": {

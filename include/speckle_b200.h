@@ -81,6 +81,30 @@ int64_t sb_last_launch_count(const sb_context *ctx);
  * [2] large amplitude try, [3] Gaussian fits, [4] bookkeeping (select, fill,
  * finalize); and the number of points each of [0..2] processed in [5..7]. */
 int sb_last_stage_timing(const sb_context *ctx, float ms[8]);
+/* Bound of every device-side wait of this context's kernels (the cullSTData
+ * wavefront kernel waits for the previous grid row): a wait gives up after
+ * `naps` naps of 64 ns, the kernel returns early and the call fails with
+ * SB_ERR_TIMEOUT; the context stays usable.  Default 2^26 (~4 s); 0 gives
+ * up at the first unmet check.  No reference counterpart (the reference's
+ * raster loop, Cullst/cullSTData.c:75-123, never waits). */
+int sb_set_wait_limit(sb_context *ctx, int64_t naps);
+
+/* Transform form of strack's complex stage (cmpPSWithPad + the IFFT of
+ * cmpTrackFast, Strack/speckleTrack.c:604-709).  No reference counterpart:
+ * the reference has one form, FFTW in float.
+ *   SB_FORM_FP32       FP32 FFTs on the CUDA cores (default).
+ *   SB_FORM_SPLIT_BF16 the patch DFTs as GEMMs on the tensor cores with
+ *                      operands split into hi + lo bfloat16 (three products,
+ *                      FP32 accumulation); the oversampling, the peak search
+ *                      and every decision stay FP32/FP64 as in the FP32 form.
+ *                      Used where supported -- complex window 64, no
+ *                      baseline, no interferogram, no -gauss -- and the FP32
+ *                      form otherwise; sb_last_form() tells which one ran. */
+#define SB_FORM_FP32 0
+#define SB_FORM_SPLIT_BF16 1
+int sb_set_form(sb_context *ctx, int form);
+/* Form the complex stage of the last sb_strack call ran (SB_FORM_*). */
+int sb_last_form(const sb_context *ctx);
 
 /* ------------------------------------------------------------------------ */
 /* Inputs                                                                    */
@@ -330,18 +354,24 @@ int sb_cullls(sb_context *ctx, const sb_cullls_params *p, sb_cullls_data *d);
  *
  * All pointers are device pointers.  patches1/patches2: nPatch patches of
  * wa x wa complex float32 (re, im interleaved, native byte order), patch k at
- * offset k*wa*wa*2 floats.  azShift: per-patch spectral roll in rows
- * (0 <= roll < wa), or NULL to estimate it from each pair as estDopCarrier1
- * does.  Outputs per patch: haveData (1 when the zero-count and empty-patch
- * tests pass), cMax (normalised correlation; -1 when the peak is too close
- * to the edge), iMax/jMax (peak in 1/NOVER-sample units, or -1000).
+ * offset k*wa*wa*2 floats.  azShift: per-patch spectral roll in rows (any
+ * integer; it is reduced modulo wa, as a roll is periodic in wa), or NULL to
+ * estimate it from each pair as estDopCarrier1 does.  Outputs per patch:
+ * haveData (1 when the zero-count and empty-patch tests pass), cMax
+ * (normalised correlation; -1 when the peak is too close to the edge),
+ * iMax/jMax (peak in 1/NOVER-sample units, or -1000).
  * wa must be 16, 24, 32, 48 or 64 (SB_NOALLOC_MAX_WA); larger windows are
- * rejected with SB_ERR_ARG.  The first call on a device looks up the
- * workspace address for that device, so make it before any stream capture.
- * Every call shares the one workspace: calls that overlap on the GPU (other
- * threads, other contexts on the same device) race and must be serialised by
- * the caller.  The workspace keeps the last call's contents; every element is
- * written before it is read, so nothing needs clearing. */
+ * rejected with SB_ERR_ARG.
+ * Set-up: sb_context_create loads this entry point's kernels and its
+ * workspace on the context's device (CUDA loads modules lazily; the
+ * workspace is allocated when its module loads), once per device and
+ * process.  A caller that reserves the GPU's memory for its own pool creates
+ * its context first; the calls themselves load no code and allocate nothing.
+ * Every call looks the workspace's device address up in the current CUDA
+ * context.  Every call shares the one workspace: calls that overlap on the
+ * GPU (other threads, other contexts on the same device) race and must be
+ * serialised by the caller.  The workspace keeps the last call's contents;
+ * every element is written before it is read, so nothing needs clearing. */
 #define SB_NOALLOC_MAX_WA 64
 #define SB_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
 int sb_amp_match_noalloc(sb_context *ctx, const float *patches1, const float *patches2, int32_t nPatch,

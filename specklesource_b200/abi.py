@@ -13,6 +13,8 @@ SB_ERR_NOMEM = -3
 SB_ERR_UNSUPPORTED = -4
 SB_ERR_NODEVICE = -5
 SB_ERR_TIMEOUT = -6
+SB_FORM_FP32 = 0
+SB_FORM_SPLIT_BF16 = 1
 
 SB_LARGEINT = 2000000000
 SB_BAD, SB_CMATCH, SB_AMPMATCH, SB_AMPMATCHLARGE = 0, 1, 2, 3
@@ -238,6 +240,9 @@ class TrackParams:
         self.initOffsets = None  # dict(nr, na, r0, a0, deltaR, deltaA, dr, da)
         self.mask = None  # dict(r0, a0, nr, na, nrl, nal, mask)
         self.intf = None  # dict(data=int16 (na, nr, 2) array, nrl, nal[, byteOrder])
+        # dict(Bn, Bp, dBn, dBp, dBnQ, dBpQ, lambda_, sinThetaD, cosThetaD, overRange): the
+        # baseparams terms and initPhaseCorrect's per-range-sample tables (speckleTrack.c:1556-1625)
+        self.baseline = None
         for k, v in kw.items():
             if not hasattr(self, k):
                 raise TypeError(f"unknown track parameter {k!r}")
@@ -269,6 +274,13 @@ class TrackParams:
                         int(m["nal"]), ptr(mk))
             keep += [mk, sm]
             p.mask = C.pointer(sm)
+        if self.baseline is not None:
+            bl = self.baseline
+            tabs = [np.ascontiguousarray(bl[k], dtype=np.float64) for k in ("sinThetaD", "cosThetaD", "overRange")]
+            sb = SbBaseline(*[float(bl[k]) for k in ("Bn", "Bp", "dBn", "dBp", "dBnQ", "dBpQ", "lambda_")],
+                            *[ptr(t) for t in tabs])
+            keep += tabs + [sb]
+            p.baseline = C.pointer(sb)
         if self.intf is not None:
             f = self.intf
             d = f["data"]

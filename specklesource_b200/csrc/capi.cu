@@ -100,6 +100,11 @@ extern "C" int sb_context_create(int device, sb_context** out)
     for (int k = 0; k < 4; ++k) cudaEventCreate(&c->ev[k]);
     for (int k = 0; k < 16; ++k) cudaEventCreate(&c->sev[k]);
     for (int k = 0; k < SB_MAX_BANDS; ++k) cudaEventCreateWithFlags(&c->chunkEv[k], cudaEventDisableTiming);
+    // Load sb_amp_match_noalloc's module (with its fixed workspace) and kernels
+    // now, so that entry point never loads code or allocates inside its calls.
+    // A failure here only disables that entry point; it reports the error.
+    c->noallocPrep = sb_noalloc_prepare();
+    if (c->noallocPrep != cudaSuccess) cudaGetLastError();
     *out = c;
     return SB_OK;
 }
@@ -121,6 +126,24 @@ extern "C" void sb_context_destroy(sb_context* c)
     cudaStreamDestroy(c->stream);
     delete c;
 }
+
+extern "C" int sb_set_wait_limit(sb_context* c, int64_t naps)
+{
+    if (!c) return SB_ERR_ARG;
+    if (naps < 0) return sb_ctx_fail(c, SB_ERR_ARG, "wait limit must be >= 0");
+    c->waitNaps = (long long)naps;
+    return SB_OK;
+}
+
+extern "C" int sb_set_form(sb_context* c, int form)
+{
+    if (!c) return SB_ERR_ARG;
+    if (form != SB_FORM_FP32 && form != SB_FORM_SPLIT_BF16) return sb_ctx_fail(c, SB_ERR_ARG, "unknown form %d", form);
+    c->form = form;
+    return SB_OK;
+}
+
+extern "C" int sb_last_form(const sb_context* c) { return c ? c->lastForm : SB_FORM_FP32; }
 
 extern "C" const char* sb_last_error(const sb_context* c)
 {
@@ -618,6 +641,8 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
     CK(launch_rec_init(drec, n, c->stream), "rec_init");
     c->launches++;
     CK(cudaMemsetAsync(dstats, 0, sizeof(unsigned long long) * 8, c->stream), "memset");
+    int* tcErrFlag = nullptr;  // set when the split-BF16 form ran
+    c->lastForm = SB_FORM_FP32;
     if (nC > 0) {
         CmplxArgs a;
         memset(&a, 0, sizeof(a));
@@ -669,7 +694,19 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
         }
         if (!a.twW || !a.tau || !a.osA || !a.osD || (p->hanningFlag && !a.hanning))
             return sb_ctx_fail(c, SB_ERR_NOMEM, "table allocation failed");
-        int bpsm = cmplx_blocks_per_sm(W);
+        // the split-BF16 tensor-core form where it applies (see sb_set_form)
+        const bool tcForm = c->form == SB_FORM_SPLIT_BF16 && cmplx_tc_supported(W) && !baseOn && !p->intf &&
+                            !p->gaussFlag && c->smMajor >= 10;
+        c->lastForm = tcForm ? SB_FORM_SPLIT_BF16 : SB_FORM_FP32;
+        int* dTcErr = nullptr;
+        if (tcForm) {
+            dTcErr = (int*)sb_ctx_buf(c, "tcErr", sizeof(int), &e);
+            if (!dTcErr) return sb_ctx_fail(c, SB_ERR_NOMEM, "device allocation failed");
+            CK(cudaMemsetAsync(dTcErr, 0, sizeof(int), c->stream), "memset");
+            a.tcErr = dTcErr;
+            tcErrFlag = dTcErr;
+        }
+        int bpsm = tcForm ? cmplx_tc_blocks_per_sm() : cmplx_blocks_per_sm(W);
         if (bpsm <= 0) return sb_ctx_fail(c, SB_ERR_CUDA, "complex kernel cannot be resident (W=%d)", W);
         // per-band sub-lists (one band: the list as planned)
         std::vector<int> bandOff(bands.nb + 1, 0);
@@ -708,7 +745,10 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
                 ak.nList = cnt;
                 ak.peak = dpeak;
                 const int nCta = c->numSM * bpsm < cnt ? c->numSM * bpsm : cnt;
-                CK(launch_strack_cmplx(W, ak, nCta, c->stream), "strack_cmplx");
+                if (tcForm)
+                    CK(launch_strack_cmplx_tc(ak, nCta, c->stream), "strack_cmplx_tc");
+                else
+                    CK(launch_strack_cmplx(W, ak, nCta, c->stream), "strack_cmplx");
                 c->launches++;
                 if (dpeak) {
                     PeakArgs pk;
@@ -746,6 +786,11 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
         cudaEventElapsedTime(&t1, c->sev[1], c->sev[2]);
         c->stage[0] = t0;
         c->stage[3] += t1;
+        if (tcErrFlag) {
+            int bad = 0;
+            CK(cudaMemcpy(&bad, tcErrFlag, sizeof(int), cudaMemcpyDeviceToHost), "tcErr");
+            if (bad) return sb_ctx_fail(c, SB_ERR_TIMEOUT, "split-BF16 complex stage: a tensor-core wait timed out");
+        }
     }
     for (int stage = 1; stage <= 2 && stage <= p->maxTries; ++stage) {
         CK(launch_select(dplan, drec, n, w, stage, dkey, c->stream), "select");

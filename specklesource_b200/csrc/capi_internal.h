@@ -31,6 +31,10 @@ struct sb_context {
     std::string err;
     std::map<std::string, DevBuf> bufs;   // grown on demand, reused across calls
     std::map<std::string, void*> tables;  // constant tables
+    cudaError_t noallocPrep = cudaSuccess;  // result of sb_noalloc_prepare at creation
+    long long waitNaps = 1LL << 26;  // bounded device waits: 64 ns naps per wait (~4 s)
+    int form = SB_FORM_FP32;         // transform form of the complex stage (sb_set_form)
+    int lastForm = SB_FORM_FP32;     // form the last sb_strack call's complex stage ran
 };
 
 int sb_ctx_fail(sb_context* c, int code, const char* fmt, ...);
@@ -38,3 +42,6 @@ int sb_ctx_cuda(sb_context* c, cudaError_t e, const char* what);
 void* sb_ctx_buf(sb_context* c, const char* name, size_t bytes, cudaError_t* err);
 int sb_image_to_device(sb_context* c, const sb_image* im, const char* name, const void** dptr);
 const float2* tw_table(sb_context* c, int N);
+// Loads the allocation-free entry point's kernels and its file-scope workspace
+// on the current device (noalloc.cu).
+cudaError_t sb_noalloc_prepare();

@@ -953,7 +953,7 @@ int run_st_data(sb_context* c, const CullJob& p, const CullDev* v, int64_t* nCul
     int warps = c->numSM * 32;
     if (warps > p.nA) warps = p.nA;
     const int threads = 128, blocks = (warps * 32 + threads - 1) / threads;
-    const long long spinLimit = 1LL << 26;  // ~4 s of 64 ns naps per wait
+    const long long spinLimit = c->waitNaps;  // 64 ns naps per wait (sb_set_wait_limit)
     switch (nv) {
     case 1: cull_median_kernel<1><<<blocks, threads, 0, s>>>(a, spinLimit); break;
     case 2: cull_median_kernel<2><<<blocks, threads, 0, s>>>(a, spinLimit); break;

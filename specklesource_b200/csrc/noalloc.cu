@@ -9,8 +9,6 @@
 // CTA, and the per-CTA workspace is a slice of g_noalloc_scratch.
 #include <cuda_runtime.h>
 
-#include <mutex>
-
 #include "capi_internal.h"
 #include "strack_device.cuh"
 
@@ -130,8 +128,8 @@ __global__ void __launch_bounds__(NoallocCfg<WS>::NT) amp_noalloc_kernel(Noalloc
             block_allsum<4, NT>(d, red);
             az = dop_shift(d[0], d[1], d[2], d[3], WS, WS);
         } else {
-            az = a.azShift[k];
-            if (az < 0 || az >= WS) az = 0;
+            az = a.azShift[k] % WS;  // a roll is periodic in wa
+            if (az < 0) az += WS;
         }
         __syncthreads();
         sbfft::fft2d_staged<WS, -1, NT>(F1, tile, twWs, nullptr);
@@ -288,9 +286,22 @@ static cudaError_t launch_noalloc(const NoallocArgs& a, int numSM, cudaStream_t 
 
 using namespace sbk;
 
-// Device address of the workspace, looked up once per device.
-static std::mutex g_noalloc_mu;
-static void* g_noalloc_ptr[64];
+// Loads this file's module (which allocates g_noalloc_scratch on the current
+// device) and all five kernel instances, so that neither happens inside a
+// later sb_amp_match_noalloc call.  Called by sb_context_create with the
+// context's device current.
+cudaError_t sb_noalloc_prepare()
+{
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    cudaFuncAttributes fa;
+    if ((e = cudaFuncGetAttributes(&fa, amp_noalloc_kernel<16>)) != cudaSuccess) return e;
+    if ((e = cudaFuncGetAttributes(&fa, amp_noalloc_kernel<24>)) != cudaSuccess) return e;
+    if ((e = cudaFuncGetAttributes(&fa, amp_noalloc_kernel<32>)) != cudaSuccess) return e;
+    if ((e = cudaFuncGetAttributes(&fa, amp_noalloc_kernel<48>)) != cudaSuccess) return e;
+    return cudaFuncGetAttributes(&fa, amp_noalloc_kernel<64>);
+}
 
 extern "C" int sb_amp_match_noalloc(sb_context* c, const float* patches1, const float* patches2, int32_t nPatch,
                                     int32_t wa, const int32_t* azShift, double* cMax, int32_t* iMax, int32_t* jMax,
@@ -306,20 +317,18 @@ extern "C" int sb_amp_match_noalloc(sb_context* c, const float* patches1, const 
         return sb_ctx_fail(c, SB_ERR_ARG, "wa=%d exceeds the allocation-free maximum %d", wa, SB_NOALLOC_MAX_WA);
     if (wa != 16 && wa != 24 && wa != 32 && wa != 48 && wa != 64)
         return sb_ctx_fail(c, SB_ERR_ARG, "wa=%d not supported (16, 24, 32, 48 or 64)", wa);
-    cudaError_t e = cudaSetDevice(c->device);
+    int nDev = 0;
+    cudaError_t e = cudaGetDeviceCount(&nDev);
+    if (e != cudaSuccess) return sb_ctx_cuda(c, e, "cudaGetDeviceCount");
+    if (c->device < 0 || c->device >= nDev) return sb_ctx_fail(c, SB_ERR_ARG, "device ordinal out of range");
+    e = cudaSetDevice(c->device);
     if (e != cudaSuccess) return sb_ctx_cuda(c, e, "cudaSetDevice");
-    if (c->device < 0 || c->device >= 64) return sb_ctx_fail(c, SB_ERR_ARG, "device ordinal out of range");
+    if (c->noallocPrep != cudaSuccess) return sb_ctx_cuda(c, c->noallocPrep, "loading the allocation-free kernels");
+    // The array's device address, looked up in the current CUDA context on
+    // every call (the module is loaded already, so this allocates nothing).
     void* scratch = nullptr;
-    {
-        std::lock_guard<std::mutex> lk(g_noalloc_mu);
-        if (!g_noalloc_ptr[c->device]) {
-            void* p = nullptr;
-            e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-            if (e != cudaSuccess) return sb_ctx_cuda(c, e, "cudaGetSymbolAddress(workspace)");
-            g_noalloc_ptr[c->device] = p;
-        }
-        scratch = g_noalloc_ptr[c->device];
-    }
+    e = cudaGetSymbolAddress(&scratch, g_noalloc_scratch);
+    if (e != cudaSuccess) return sb_ctx_cuda(c, e, "cudaGetSymbolAddress(workspace)");
     NoallocArgs a;
     a.p1 = reinterpret_cast<const float2*>(patches1);
     a.p2 = reinterpret_cast<const float2*>(patches2);

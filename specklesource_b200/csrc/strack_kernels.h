@@ -67,6 +67,9 @@ struct CmplxArgs {
     const float2* twP;          // exp(-2 pi i e / ps), e < ps
     int gauss;                  // -gauss: 2-D Gaussian fit instead of the oversampling
     PeakJob* peak;              // one entry per list position (unused with -gauss)
+    // split-BF16 form only
+    int* tcErr;                 // set when a bounded wait on the tensor cores gave up
+    float* tcDebug;             // non-null: |c|^2 planes of list entry 0 (4 x 64 x 64)
 };
 
 // Arguments of an amplitude try (small: s = 1, large: s = LA = 2).
@@ -102,6 +105,11 @@ struct AmpArgs {
 bool cmplx_supported(int W);
 int cmplx_blocks_per_sm(int W);
 cudaError_t launch_strack_cmplx(int W, const CmplxArgs& a, int nCta, cudaStream_t st);
+
+// split-BF16 tensor-core form of the complex stage (strack_cmplx_tc.cu)
+bool cmplx_tc_supported(int W);
+int cmplx_tc_blocks_per_sm();
+cudaError_t launch_strack_cmplx_tc(const CmplxArgs& a, int nCta, cudaStream_t st);
 
 bool amp_supported(int Ws);
 size_t amp_scratch_elems(int Ws);

@@ -24,6 +24,9 @@ SIGNATURES = {
     "sb_last_timing": (C.c_int, [_P, C.POINTER(C.c_float)]),
     "sb_last_launch_count": (C.c_int64, [_P]),
     "sb_last_stage_timing": (C.c_int, [_P, C.POINTER(C.c_float)]),
+    "sb_set_wait_limit": (C.c_int, [_P, C.c_int64]),
+    "sb_set_form": (C.c_int, [_P, C.c_int]),
+    "sb_last_form": (C.c_int, [_P]),
     "sb_strack": (C.c_int, [_P, C.POINTER(abi.SbTrackParams), C.POINTER(abi.SbImage), C.POINTER(abi.SbImage),
                             C.POINTER(abi.SbTrackResult)]),
     "sb_strackw": (C.c_int, [_P, C.POINTER(abi.SbTrackParams), C.POINTER(abi.SbImage), C.POINTER(abi.SbImage),
@@ -142,6 +145,14 @@ class Context:
 
     def launch_count(self):
         return int(self.lib.sb_last_launch_count(self.h))
+
+    def set_form(self, form):
+        """Transform form of strack's complex stage: abi.SB_FORM_FP32 (default)
+        or abi.SB_FORM_SPLIT_BF16 (tensor cores, complex window 64)."""
+        self._check(self.lib.sb_set_form(self.h, int(form)))
+
+    def last_form(self):
+        return int(self.lib.sb_last_form(self.h))
 
     def _track(self, fn, params, img1, img2, out, azd):
         p, keep = params.to_c()

@@ -152,3 +152,26 @@ def test_cullls_large_grid(ctx):
     o = oracle.cullls(p, X, Y, t)
     _check_ls(g, o)
     assert o["nIslands"] > 0
+
+
+def test_wavefront_wait_times_out_and_context_stays_usable(ctx):
+    """The row-wavefront median kernel (13 x 13 box) waits for the previous
+    grid row with a bounded wait.  With a limit of 0 naps the first unmet
+    check gives up: the call fails with SB_ERR_TIMEOUT (nothing hangs), and the
+    same context then culls the grid bit-exactly with the default limit."""
+    from specklesource_b200.runtime import SpeckleError
+    nA, nR = 150, 230
+    offR, offA, corr, mt = offsets_field(nA, nR, 7)
+    p = abi.CullParams(nR=nR, nA=nA, bR=13, bA=13, nGood=40, islandThresh=6)
+    assert ctx.lib.sb_set_wait_limit(ctx.h, -1) == abi.SB_ERR_ARG
+    assert ctx.lib.sb_set_wait_limit(ctx.h, 0) == abi.SB_OK
+    try:
+        with pytest.raises(SpeckleError, match="timed out") as ei:
+            ctx.cull(p, offR, offA, corr, mt)
+        assert ei.value.code == abi.SB_ERR_TIMEOUT
+    finally:
+        assert ctx.lib.sb_set_wait_limit(ctx.h, 1 << 26) == abi.SB_OK
+    g = ctx.cull(p, offR, offA, corr, mt)
+    o = oracle.cull(p, offR, offA, corr, mt)
+    _check(g, o)
+    assert g["nCulled"] == o["nCulled"]

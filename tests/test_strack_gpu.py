@@ -221,3 +221,39 @@ def test_gauss_fit_moderate_coherence(ctx):
     p = _p(rStart=72, aStart=72, nR=24, nA=24, deltaR=16, deltaA=16, gaussFlag=1)
     g, o, st = _check(ctx, p, a, b)
     assert o["stats"]["nAmp"] > 20 and o["stats"]["nAmpL"] > 100 and o["stats"]["nComplex"] > 100
+
+
+def _baseline_tables(nr, ramp, lam=0.0555):
+    """Per-range-sample tables of initPhaseCorrect (speckleTrack.c:1556-1625)
+    chosen so that phaseCorrectBaseline's dominant term, -bn sinThetaD ptod,
+    is a range ramp of `ramp` rad/px for bn = 1; the cosThetaD and overRange
+    terms add small, slowly varying phases so that every term is exercised."""
+    ptod = -(4.0 * np.pi) / lam
+    j = np.arange(nr, dtype=np.float64)
+    sin_t = -ramp * j / ptod + 1e-4 * np.sin(j / 50.0)
+    cos_t = 0.9 + 1e-6 * j
+    over_r = 1.0 / (850e3 + 2.33 * j)
+    return sin_t, cos_t, over_r
+
+
+def test_baseline_phase_flattening(ctx):
+    """phaseCorrectBaseline (speckleTrack.c:868-907) with a non-zero baseline:
+    image 2 carries a 0.6 rad/px range fringe that decorrelates the pair; the
+    baseline terms (Bn, Bp, dBn, dBp, dBnQ, dBpQ all non-zero) put the same
+    fringe on patch 1, so complex matching recovers.  GPU against the oracle
+    at the usual bar, at W = 32 and 64."""
+    import torch
+    s1, s2 = synth.make_pair(512, 1024, 12, dr=lambda y, x: 1.3 + 0.3 * torch.sin(x / 150.0),
+                             da=lambda y, x: 0.4 + 0 * x, coherence=0.8, ramp=0.6)
+    a, b = synth.to_numpy(s1), synth.to_numpy(s2)
+    sin_t, cos_t, over_r = _baseline_tables(1024, 0.6)
+    base = dict(Bn=1.0, Bp=2.0, dBn=0.02, dBp=0.3, dBnQ=0.01, dBpQ=0.05, lambda_=0.0555,
+                sinThetaD=sin_t, cosThetaD=cos_t, overRange=over_r)
+    for W in (32, 64):
+        kw = dict(rStart=W + 8, aStart=W + 8, deltaR=W // 2, deltaA=W // 2, nR=(1024 - 2 * W - 16) // (W // 2),
+                  nA=(512 - 2 * W - 16) // (W // 2), wR=W, wA=W, wRa=W, wAa=W)
+        p = abi.TrackParams(**kw, baseline=base)
+        g, o, st = _check(ctx, p, a, b)
+        assert (o["type"] == 1).mean() > 0.9 and (g["type"] == 1).mean() > 0.9
+        plain = oracle.strack(abi.TrackParams(**kw), a, b)
+        assert (plain["type"] == 1).mean() < 0.3  # without the baseline the fringe decorrelates the pair

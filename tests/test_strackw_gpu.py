@@ -98,3 +98,23 @@ def test_est_dop_carrier_batch(ctx):
     assert rc == abi.SB_OK
     want = [oracle.est_dop_carrier(P1[k], P2[k], nAz) for k in range(n)]
     assert out.cpu().numpy().tolist() == want
+
+
+def test_strackw_config3_geometry_240_points():
+    """The benchmark's fast-flow geometry (search window 224 = 128 + 2 x 48,
+    edge pad 48, 5 x 5 box pre-smoothing) on 240 points spread over a
+    2000 x 4000 pair of the shear-zone generator (|d| up to 40 px, coherence
+    0.25-0.5), against the FP64 oracle."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from specklesource_b200 import build, runtime
+    build.build()
+    s1, s2 = synth.shear_pair(device="cuda", na=2000, nr=4000, seed=3)
+    a, b = synth.to_numpy(s1), synth.to_numpy(s2)
+    del s1, s2
+    p = abi.TrackParams(rStart=160, aStart=160, deltaR=160, deltaA=140, nR=20, nA=12, wR=224, wA=224, wRa=224,
+                        wAa=224, edgePadR=48, edgePadA=48, navgR=2, navgA=2)
+    with runtime.Context(0) as c:
+        g, o = _check(c, p, a, b)
+    assert (o["type"] == abi.SB_AMPMATCH).sum() >= 200
