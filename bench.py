@@ -44,7 +44,7 @@ N_R = (NR - 2 * GRID["rStart"]) // GRID["deltaR"] + 1  # 993
 N_A = (NA - 2 * GRID["aStart"]) // GRID["deltaA"] + 1  # 1969
 
 
-METRIC = "patches/s at <=0.02 px err vs FP64 oracle (plain FP32); p50/p99 ms"
+METRIC = "patches/s at <=0.02 px err vs FP64 oracle (plain FP32 vs split-BF16); p50/p99 ms"
 
 
 def use_small_workload():
@@ -318,6 +318,23 @@ def accuracy_vs_fp64(img1, img2, gpu, rows_per_worker=1, workers=None):
         pairs.append(({k: gpu[k][sl] for k in ("offR", "offA", "corr", "type")}, o))
     out = _accuracy_blocks(pairs)
     out["sample"] = f"{workers} x {rows_per_worker} grid rows spread over the grid, FP64 oracle, {wall:.1f} s"
+    return out
+
+
+def accuracy_vs_fp64_forms(img1, img2, gpu_by_form, rows_per_worker=1, workers=None):
+    """accuracy_vs_fp64 for several GPU outputs of the same workload (one per
+    transform form) against one FP64 oracle run."""
+    workers = workers or os.cpu_count()
+    jobs, starts = _row_jobs(img1, img2, rows_per_worker, workers, "f64")
+    res, wall = _run_pool(jobs)
+    out = {}
+    for name, gpu in gpu_by_form.items():
+        pairs = []
+        for (_, _, o), i0 in zip(res, starts):
+            sl = slice(i0, i0 + rows_per_worker)
+            pairs.append(({k: gpu[k][sl] for k in ("offR", "offA", "corr", "type")}, o))
+        out[name] = _accuracy_blocks(pairs)
+        out[name]["sample"] = f"{workers} x {rows_per_worker} grid rows spread over the grid, FP64 oracle, {wall:.1f} s"
     return out
 
 
@@ -809,6 +826,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp32-peak", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the FP64-oracle check of a row sample")
+    ap.add_argument("--form", default="fp32", choices=["fp32", "split-bf16"],
+                    help="transform form of the complex stage timed for the headline value; the other form is "
+                         "measured beside it")
+    ap.add_argument("--no-other-form", action="store_true", help="skip measuring the other transform form")
     ap.add_argument("--slots", type=int, default=4, help="job-server slots for --workload cfg4/cfg5")
     ap.add_argument("--jobs", type=int, default=200, help="jobs offered in --workload cfg5")
     ap.add_argument("--batch", type=int, default=32768, help="patches per batch in --workload dftgemm")
@@ -835,7 +856,10 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     from specklesource_b200 import runtime, synth
 
+    from specklesource_b200 import abi
     ctx = runtime.Context(local)
+    forms = {"fp32": abi.SB_FORM_FP32, "split-bf16": abi.SB_FORM_SPLIT_BF16}
+    ctx.set_form(forms[args.form])
     p = track_params()
     s1, s2 = synth.large_pair(device="cuda", na=NA, nr=NR, seed=replica_seed(rank))
     torch.cuda.synchronize()
@@ -870,7 +894,32 @@ def main():
     ms_step = max_over_ranks(torch, tot_ms / args.steps, world, "cuda")
     value = job_rate(world, n_pts, ms_step)
 
-    # ---- roofline of the dominant kernel (complex stage, FP32 CUDA cores)
+    form_ran = ctx.last_form()
+    outputs = {args.form: {k: out[k].cpu().numpy() for k in ("offR", "offA", "corr", "type")}}
+    form_stats = {args.form: {"ms_per_call": ms_step, "patches_per_s": value,
+                              "cmplx_ms": float(np.mean([s_["cmplx_ms"] for s_ in stages])),
+                              "ran": "split-bf16" if form_ran == abi.SB_FORM_SPLIT_BF16 else "fp32"}}
+    if not args.no_other_form:
+        other = "split-bf16" if args.form == "fp32" else "fp32"
+        ctx.set_form(forms[other])
+        for _ in range(max(2, args.warmup)):
+            step_dev()
+        barrier()
+        o_ms, o_cm = [], []
+        for _ in range(args.steps):
+            t, st, _ = step_dev()
+            o_ms.append(t)
+            o_cm.append(st["cmplx_ms"])
+        barrier()
+        om = max_over_ranks(torch, float(np.mean(o_ms)), world, "cuda")
+        form_stats[other] = {"ms_per_call": om, "patches_per_s": job_rate(world, N_A * N_R, om),
+                             "cmplx_ms": float(np.mean(o_cm)),
+                             "ran": "split-bf16" if ctx.last_form() == abi.SB_FORM_SPLIT_BF16 else "fp32"}
+        outputs[other] = {k: out[k].cpu().numpy() for k in ("offR", "offA", "corr", "type")}
+        ctx.set_form(forms[args.form])
+
+    # ---- roofline of the dominant kernel (complex stage: FP32 CUDA cores, or
+    # the tensor cores for the split-BF16 form)
     st0 = stages[-1]
     cm_ms = float(np.mean([s["cmplx_ms"] for s in stages]))
     ach_tflops = st0["n_cmplx"] * ALG_CMPLX / (cm_ms * 1e-3) / 1e12
@@ -906,12 +955,53 @@ def main():
         if not args.no_cpu_baseline:
             cpu = cpu_baseline(a, b, rows_per_worker=args.cpu_rows)
         if not args.no_accuracy:
-            g = {k: out[k].cpu().numpy() for k in ("offR", "offA", "corr", "type")}
-            acc = accuracy_vs_fp64(a, b, g)
+            acc_forms = accuracy_vs_fp64_forms(a, b, outputs)
+            acc = acc_forms[args.form]
+            for name, st_ in form_stats.items():
+                st_["accuracy"] = acc_forms[name]
             del a, b
             parity = parity_other_configs(ctx)
-    key = f"strack_cmplx_w64_{NA}x{NR}"
-    traffic = measured_traffic(key)
+    if args.form == "split-bf16":
+        # the split-BF16 kernel is bound by the tensor pipe: GEMM flops per patch
+        # = 6 passes x 3 products x 2 x 128 x 128 x 128 (real block form)
+        key = f"strack_cmplx_tc_w64_{NA}x{NR}"
+        traffic = measured_traffic(key)
+        gemm = 6 * 3 * 2.0 * 128 ** 3
+        ach = st0["n_cmplx"] * gemm / (cm_ms * 1e-3) / 1e12
+        tpk = peaks.get("bf16_tflops_sustained") or peaks.get("bf16_tflops")
+        roofline = {
+            "bound": "tensor", "achieved": ach, "peak": tpk, "unit": "TFLOP/s", "frac": ach / tpk,
+            "peak_source": f"MEASURED_PEAKS.json bf16 dense, sustained ({src}); the complex stage runs inside "
+                           "back-to-back calls",
+            "gemm_flops_per_patch": gemm, "alg_flops_per_patch": ALG_CMPLX,
+            "alg_tflops": ach_tflops, "alg_frac_of_fp32": ach_tflops / fp32,
+            "traffic": traffic,
+            "traffic_source": f"ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, profiles/{key}.md"
+                              if traffic else "no committed capture for this workload",
+            "launch_patches": min(n_pts, PEAK_CHUNK), "launches_per_call": -(-n_pts // PEAK_CHUNK),
+            "alg_bytes_per_launch": int((img_bytes + n_pts * (4 * 4 + 1)) * min(n_pts, PEAK_CHUNK) / n_pts),
+            "kernel": "strack_cmplx_tc_kernel (tcgen05, M128 N64 K16 bf16, 144 MMAs per patch)",
+            "hbm": {"achieved_gbs": img_bytes / (cm_ms * 1e-3) / 1e9, "peak_gbs": peaks.get("hbm_gbs"),
+                    "peak_source": src},
+        }
+    else:
+        key = f"strack_cmplx_w64_{NA}x{NR}"
+        traffic = measured_traffic(key)
+        roofline = {
+            "bound": "fp32", "achieved": ach_tflops, "peak": fp32, "unit": "TFLOP/s",
+            "frac": ach_tflops / fp32,
+            "traffic": traffic,
+            "traffic_source": f"ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, profiles/{key}.md"
+                              if traffic else "no committed capture for this workload",
+            "launch_patches": min(n_pts, PEAK_CHUNK),
+            "launches_per_call": -(-n_pts // PEAK_CHUNK),
+            "alg_bytes_per_launch": int((img_bytes + n_pts * (4 * 4 + 1)) * min(n_pts, PEAK_CHUNK) / n_pts),
+            "kernel": "strack_cmplx_kernel<64,256>",
+            "alg_flops_per_patch": ALG_CMPLX,
+            "peak_source": "cuBLAS SGEMM 8192^3 (TF32 off) measured in this run",
+            "hbm": {"achieved_gbs": (img_bytes) / (cm_ms * 1e-3) / 1e9, "peak_gbs": peaks.get("hbm_gbs"),
+                    "peak_source": src},
+        }
 
     if rank == 0:
         line = {
@@ -927,21 +1017,9 @@ def main():
             "parity_other_configs": parity,
             "gpu_launches": launches,
             "stages": {k: float(np.mean([s[k] for s in stages])) for k in stages[-1]},
-            "roofline": {
-                "bound": "fp32", "achieved": ach_tflops, "peak": fp32, "unit": "TFLOP/s",
-                "frac": ach_tflops / fp32,
-                "traffic": traffic,
-                "traffic_source": f"ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, profiles/{key}.md"
-                                  if traffic else "no committed capture for this workload",
-                "launch_patches": min(n_pts, PEAK_CHUNK),
-                "launches_per_call": -(-n_pts // PEAK_CHUNK),
-                "alg_bytes_per_launch": int((img_bytes + n_pts * (4 * 4 + 1)) * min(n_pts, PEAK_CHUNK) / n_pts),
-                "kernel": "strack_cmplx_kernel<64,256>",
-                "alg_flops_per_patch": ALG_CMPLX,
-                "peak_source": "cuBLAS SGEMM 8192^3 (TF32 off) measured in this run",
-                "hbm": {"achieved_gbs": (img_bytes) / (cm_ms * 1e-3) / 1e9, "peak_gbs": peaks.get("hbm_gbs"),
-                        "peak_source": src},
-            },
+            "form": args.form,
+            "forms": form_stats,
+            "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clk,
         }

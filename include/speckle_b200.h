@@ -106,6 +106,15 @@ int sb_set_form(sb_context *ctx, int form);
 /* Form the complex stage of the last sb_strack call ran (SB_FORM_*). */
 int sb_last_form(const sb_context *ctx);
 
+/* Device memory the context holds (bytes): the buffers its calls grew, kept
+ * for reuse by later calls, and its constant tables.  No reference
+ * counterpart (the reference mallocs per run and never frees). */
+int64_t sb_context_device_bytes(const sb_context *ctx);
+/* Frees the context's grown buffers (after its stream is idle); later calls
+ * grow them again.  The constant tables are kept.  For a server that admits
+ * jobs against a device-memory budget.  No reference counterpart. */
+int sb_context_release(sb_context *ctx);
+
 /* ------------------------------------------------------------------------ */
 /* Inputs                                                                    */
 /* ------------------------------------------------------------------------ */

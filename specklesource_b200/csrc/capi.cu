@@ -135,6 +135,27 @@ extern "C" int sb_set_wait_limit(sb_context* c, int64_t naps)
     return SB_OK;
 }
 
+extern "C" int64_t sb_context_device_bytes(const sb_context* c)
+{
+    if (!c) return 0;
+    size_t b = c->tableBytes;
+    for (const auto& kv : c->bufs) b += kv.second.bytes;
+    return (int64_t)b;
+}
+
+extern "C" int sb_context_release(sb_context* c)
+{
+    if (!c) return SB_ERR_ARG;
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) return sb_ctx_cuda(c, e, "cudaSetDevice");
+    cudaStreamSynchronize(c->stream);
+    cudaStreamSynchronize(c->copyStream);
+    for (auto& kv : c->bufs)
+        if (kv.second.ptr) cudaFree(kv.second.ptr);
+    c->bufs.clear();
+    return SB_OK;
+}
+
 extern "C" int sb_set_form(sb_context* c, int form)
 {
     if (!c) return SB_ERR_ARG;
@@ -178,6 +199,7 @@ const void* sb_table(sb_context* c, const std::string& key, const std::vector<fl
     if (cudaMalloc(&d, host.size() * sizeof(float2)) != cudaSuccess) return nullptr;
     cudaMemcpy(d, host.data(), host.size() * sizeof(float2), cudaMemcpyHostToDevice);
     c->tables[key] = d;
+    c->tableBytes += host.size() * sizeof(float2);
     return d;
 }
 

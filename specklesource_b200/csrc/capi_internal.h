@@ -31,6 +31,7 @@ struct sb_context {
     std::string err;
     std::map<std::string, DevBuf> bufs;   // grown on demand, reused across calls
     std::map<std::string, void*> tables;  // constant tables
+    size_t tableBytes = 0;                // device bytes of the tables
     cudaError_t noallocPrep = cudaSuccess;  // result of sb_noalloc_prepare at creation
     long long waitNaps = 1LL << 26;  // bounded device waits: 64 ns naps per wait (~4 s)
     int form = SB_FORM_FP32;         // transform form of the complex stage (sb_set_form)

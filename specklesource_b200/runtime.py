@@ -26,6 +26,8 @@ SIGNATURES = {
     "sb_last_stage_timing": (C.c_int, [_P, C.POINTER(C.c_float)]),
     "sb_set_wait_limit": (C.c_int, [_P, C.c_int64]),
     "sb_set_form": (C.c_int, [_P, C.c_int]),
+    "sb_context_device_bytes": (C.c_int64, [_P]),
+    "sb_context_release": (C.c_int, [_P]),
     "sb_last_form": (C.c_int, [_P]),
     "sb_strack": (C.c_int, [_P, C.POINTER(abi.SbTrackParams), C.POINTER(abi.SbImage), C.POINTER(abi.SbImage),
                             C.POINTER(abi.SbTrackResult)]),
@@ -145,6 +147,14 @@ class Context:
 
     def launch_count(self):
         return int(self.lib.sb_last_launch_count(self.h))
+
+    def device_bytes(self):
+        """Device memory this context holds (grown buffers + tables), bytes."""
+        return int(self.lib.sb_context_device_bytes(self.h))
+
+    def release(self):
+        """Frees the context's grown buffers (they grow again on the next call)."""
+        self._check(self.lib.sb_context_release(self.h))
 
     def set_form(self, form):
         """Transform form of strack's complex stage: abi.SB_FORM_FP32 (default)

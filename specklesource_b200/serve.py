@@ -6,8 +6,9 @@ A job is one image pair tracked with `strack` (Strack/speckleTrack.c) or
 (Cullst/cullst.c:71-101) on its offsets grid.  The server owns `slots` library
 contexts; each has its own CUDA stream and reusable device buffers and is
 driven by its own host thread, so jobs on different slots overlap on the GPU
-(the C calls release the GIL).  A job starts when a slot is free and its
-estimated device memory fits the HBM budget; admission is first come, first
+(the C calls release the GIL).  A job starts when a slot is free and the
+device memory the slots hold or need stays within the HBM budget (see
+JobServer); admission is first come, first
 served (the head of the queue is never bypassed, so a large job cannot
 starve).  Images may be torch CUDA tensors (device-resident, nothing copied)
 or host arrays (copied inside the call).  Results are the same whether a job
@@ -91,8 +92,16 @@ def job_device_bytes(job, num_sm=148):
 
 class JobServer:
     """Continuous-batching server.  context_factory(device) -> an object with
-    the runtime.Context methods strack/strackw/cull/close (a fake one in the
-    CPU tests)."""
+    the runtime.Context methods strack/strackw/cull/close, and optionally
+    device_bytes/release (a fake one in the CPU tests).
+
+    Device-memory budget: a context keeps the buffers its calls grew (reused
+    by its next job), so the budget counts, per slot, the larger of what its
+    context holds (measured after each job with device_bytes) and the
+    estimate of the job it runs.  A job is admitted on a free slot when that
+    sum over all slots stays within the budget; when the head of the queue
+    does not fit, idle slots release their buffers first.  Images passed as
+    CUDA tensors belong to the caller and are not counted."""
 
     def __init__(self, device=0, slots=4, hbm_budget=120e9, context_factory=None, num_sm=148):
         if context_factory is None:
@@ -103,17 +112,33 @@ class JobServer:
         self._ctx = [context_factory(device) for _ in range(slots)]
         self._cv = threading.Condition()
         self._queue = collections.deque()
-        self._in_use = 0.0
+        self._held = [self._measure(c) for c in self._ctx]   # bytes each context holds
+        self._running = [0.0] * slots                          # estimate of the job on each slot
         self._peak = 0.0
         self._closed = False
+        self.releases = 0
         self.started = []  # (tag, start time) in admission order
         self._threads = [threading.Thread(target=self._worker, args=(k,), daemon=True) for k in range(slots)]
         for t in self._threads:
             t.start()
 
+    @staticmethod
+    def _measure(ctx):
+        f = getattr(ctx, "device_bytes", None)
+        return float(f()) if f else 0.0
+
     @property
     def peak_bytes(self):
+        """Largest device memory reserved at once (sum over slots of the held
+        or estimated bytes), bytes."""
         return self._peak
+
+    def reserved_bytes(self):
+        with self._cv:
+            return self._reserved()
+
+    def _reserved(self, skip=None):
+        return sum(max(h, r) for k, (h, r) in enumerate(zip(self._held, self._running)) if k != skip)
 
     def submit(self, job):
         """Queues a job; returns a Future resolving to a dict with the track
@@ -132,43 +157,59 @@ class JobServer:
             self._cv.notify_all()
         return fut
 
-    def _take(self):
+    def _take(self, k):
+        ctx = self._ctx[k]
         with self._cv:
             while True:
                 if self._closed and not self._queue:
                     return None
                 if self._queue:
                     job, need, fut = self._queue[0]
-                    if self._in_use + need <= self.budget:
+                    if self._reserved(skip=k) + max(self._held[k], need) <= self.budget:
                         self._queue.popleft()
-                        self._in_use += need
-                        self._peak = max(self._peak, self._in_use)
+                        self._running[k] = float(need)
+                        self._peak = max(self._peak, self._reserved())
                         self.started.append((job.tag, time.perf_counter()))
                         self._cv.notify_all()
                         return job, need, fut
+                    if self._held[k] > 0 and getattr(ctx, "release", None):
+                        # the head does not fit: this idle slot gives its buffers back
+                        self._cv.release()
+                        try:
+                            ctx.release()
+                        finally:
+                            self._cv.acquire()
+                        self._held[k] = self._measure(ctx)
+                        self.releases += 1
+                        self._cv.notify_all()
+                        continue
                 self._cv.wait()
 
-    def _release(self, need):
+    def _finish(self, k):
+        held = self._measure(self._ctx[k])
         with self._cv:
-            self._in_use -= need
+            self._held[k] = held
+            self._running[k] = 0.0
+            self._peak = max(self._peak, self._reserved())
             self._cv.notify_all()
 
     def _worker(self, k):
         ctx = self._ctx[k]
         while True:
-            item = self._take()
+            item = self._take(k)
             if item is None:
                 return
             job, need, fut = item
             try:
                 t0 = time.perf_counter()
                 res = run_job(ctx, job)
-                res.update(start=t0, end=time.perf_counter(), arrival=job.arrival, slot=k)
+                res.update(start=t0, end=time.perf_counter(), arrival=job.arrival, slot=k,
+                           held_bytes=self._measure(ctx))
                 fut.set_result(res)
             except Exception as e:  # reported through the future
                 fut.set_exception(e)
             finally:
-                self._release(need)
+                self._finish(k)
 
     def close(self):
         with self._cv:

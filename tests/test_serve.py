@@ -82,6 +82,50 @@ def test_job_above_budget_is_refused():
             f.result(timeout=5)
 
 
+class HoldingContext(FakeContext):
+    """A fake context that keeps device buffers after a job, like the
+    library's contexts: it holds `need` bytes once it has run a job, until
+    release() is called."""
+    log = []
+
+    def __init__(self, device):
+        super().__init__(device)
+        self.held = 0
+
+    def _run(self, p):
+        r = super()._run(p)
+        self.held = serve.job_device_bytes(_job(p.nR, p.nA))
+        HoldingContext.log.append(self.held)
+        return r
+
+    def device_bytes(self):
+        return self.held
+
+    def release(self):
+        self.held = 0
+
+
+def test_budget_counts_buffers_held_by_idle_slots():
+    """Idle slots still hold their last job's buffers and the budget counts
+    them: a job that fits only once they are freed makes the idle slots
+    release their buffers first."""
+    FakeContext.running = FakeContext.max_running = 0
+    one = serve.job_device_bytes(_job(10))
+    big = _job(200, 400)  # 80,000 points: about twice a small job's buffers
+    need_big = serve.job_device_bytes(big)
+    budget = 2.2 * one
+    assert 2 * one <= budget < one + need_big and need_big <= budget
+    with serve.JobServer(slots=2, hbm_budget=budget, context_factory=HoldingContext) as srv:
+        first = [f.result(timeout=10) for f in [srv.submit(_job(10)) for _ in range(2)]]
+        assert {r["slot"] for r in first} == {0, 1}  # both ran at once; both slots now hold buffers
+        assert srv.reserved_bytes() == 2 * one
+        r = srv.submit(big).result(timeout=10)
+        assert srv.releases >= 1  # an idle slot gave its buffers back before the big job started
+        assert srv.peak_bytes <= budget
+        assert srv.reserved_bytes() <= budget
+    assert r["track"]["offR"][0, 0] == 200
+
+
 def test_latency_stats():
     rs = [{"arrival": 0.0, "end": 0.001 * k} for k in range(1, 101)]
     st = serve.latency_stats(rs)
@@ -121,6 +165,41 @@ def test_same_result_alone_and_in_the_mix():
             assert np.array_equal(a["track"][k], m["track"][k], equal_nan=True), k
         for k in ("offRS", "offAS", "type"):
             assert np.array_equal(a["cull"][k], m["cull"][k], equal_nan=True), k
+
+
+@pytest.mark.gpu
+def test_device_memory_stays_within_the_budget():
+    """Mixed jobs under a budget that fits about one job at a time: after
+    every job the device memory all slots' contexts hold (sb_context_device_bytes)
+    is within the budget, and the results are those of the jobs run alone."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from specklesource_b200 import build, runtime, synth
+    build.build()
+    jobs = []
+    for k, (na, nr, W) in enumerate([(768, 1024, 64), (512, 768, 32), (1024, 1024, 48), (640, 896, 64),
+                                      (512, 512, 32), (896, 768, 48)]):
+        s1, s2 = synth.small_pair(device="cpu", na=na, nr=nr, seed=40 + k)
+        a, b = synth.to_numpy(s1), synth.to_numpy(s2)  # host images: their device copies count
+        p = abi.TrackParams(rStart=W, aStart=W, deltaR=W // 2, deltaA=W // 2, nR=(nr - 2 * W) // (W // 2),
+                            nA=(na - 2 * W) // (W // 2), wR=W, wA=W, wRa=W, wAa=W)
+        jobs.append(serve.Job(kind="strack", params=p, img1=a, img2=b,
+                              cull=abi.CullParams(nR=p.nR, nA=p.nA), tag=k))
+    with runtime.Context(0) as ctx:
+        alone = [serve.run_job(ctx, j) for j in jobs]
+    budget = 1.3 * max(serve.job_device_bytes(j) for j in jobs)
+    with serve.JobServer(slots=3, hbm_budget=budget) as srv:
+        futs = [srv.submit(j) for j in jobs]
+        mixed = [f.result(timeout=600) for f in futs]
+        held = [c.device_bytes() for c in srv._ctx]
+        assert sum(held) <= budget, (held, budget)
+        assert srv.peak_bytes <= budget
+        for r in mixed:  # what the job's own context held when it finished
+            assert r["held_bytes"] <= budget
+    for a, m in zip(alone, mixed):
+        for k in ("offR", "offA", "corr", "type"):
+            assert np.array_equal(a["track"][k], m["track"][k], equal_nan=True), k
 
 
 def test_estimate_counts_the_peak_hand_off_once_per_chunk():
