@@ -241,6 +241,21 @@ typedef struct {
 int sb_strack(sb_context *ctx, const sb_track_params *p, const sb_image *img1,
               const sb_image *img2, sb_track_result *out);
 
+/* Many pairs in one call: speckleTrack (as sb_strack) for nPairs image pairs,
+ * params[k], img1[k], img2[k] -> out[k].  No reference counterpart (the
+ * reference tracks one pair per run); each pair's grids and statistics equal
+ * its own sb_strack result.  The pairs are grouped by window size and every
+ * stage runs once per group over the points of all its pairs (one persistent
+ * complex-stage launch per group), which pays off for many small pairs.
+ * Pairs may differ in image size, grid, windows, initial shift and mask; the
+ * images share sample type and byte order, and the flags noComplex,
+ * hanningFlag, maxTries, checkAzFocus, gaussFlag, azDefocusThresh and
+ * scaleFactor are the same for every pair.  Baseline and interferogram
+ * flattening are refused (SB_ERR_UNSUPPORTED): use sb_strack.  The device
+ * holds both images of every pair at once (copied into two atlases). */
+int sb_strack_batch(sb_context *ctx, int32_t nPairs, const sb_track_params *params, const sb_image *img1,
+                    const sb_image *img2, sb_track_result *out);
+
 /* Replaces void corrTrackFast(TrackParams *) (Strackw/strackt.h:31,
  * body Strackw/corrTrackFast.c:89-231): normalised amplitude correlation of a
  * chip of image 2 inside a search window of image 1. */

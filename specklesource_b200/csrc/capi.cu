@@ -18,6 +18,7 @@
 #include <string.h>
 
 #include <string>
+#include <algorithm>
 #include <vector>
 
 #include "../../include/speckle_b200.h"
@@ -918,5 +919,369 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
         float tk = c->timing[2] - c->stage[0] - c->stage[1] - c->stage[2] - c->stage[3];
         c->stage[4] = tk > 0 ? tk : 0.f;
     }
+    return SB_OK;
+}
+
+// ---------------------------------------------------------------- batched strack
+// Many image pairs in one call.  The pairs are ordered by window bucket
+// (complex window, amplitude window); both images of every pair are copied
+// into two atlases (images stacked along azimuth, one row pitch), so a point's
+// windows are addressed like any single pair's and every stage kernel runs
+// once per bucket over the points of all pairs in it: one persistent complex
+// launch per bucket (and list chunk), one peak and one fit launch, then the
+// amplitude tries and the finalize pass per bucket.  Per point the arithmetic
+// is that of sb_strack, so each pair's grids equal its own sb_strack result.
+
+namespace {
+struct Bucket {
+    int wR, wRa;
+    int pFirst, pLast;           // range in the bucket order of the pairs
+    int g0, g1;                  // global point range
+    int l0, l1;                  // range of the complex list
+};
+}  // namespace
+
+extern "C" int sb_strack_batch(sb_context* c, int32_t nPairs, const sb_track_params* P, const sb_image* I1,
+                               const sb_image* I2, sb_track_result* out)
+{
+    if (!c) return SB_ERR_ARG;
+    c->err.clear();
+    c->launches = 0;
+    if (nPairs <= 0 || !P || !I1 || !I2 || !out) return sb_ctx_fail(c, SB_ERR_ARG, "empty batch or null arrays");
+    const sb_track_params& p0 = P[0];
+    int rc;
+    int64_t total = 0;
+    for (int k = 0; k < nPairs; ++k) {
+        const sb_track_params* p = &P[k];
+        if ((rc = check_image(c, &I1[k])) != SB_OK || (rc = check_image(c, &I2[k])) != SB_OK) return rc;
+        if (I1[k].sampleType != I1[0].sampleType || I2[k].sampleType != I1[0].sampleType ||
+            I1[k].byteOrder != I1[0].byteOrder || I2[k].byteOrder != I1[0].byteOrder)
+            return sb_ctx_fail(c, SB_ERR_ARG, "pair %d: every image of a batch has the same sample type and byte order",
+                               k);
+        if (p->nR <= 0 || p->nA <= 0) return sb_ctx_fail(c, SB_ERR_ARG, "pair %d: empty grid", k);
+        if (p->scaleFactor <= 0) return sb_ctx_fail(c, SB_ERR_ARG, "pair %d: scaleFactor must be positive", k);
+        if (p->polyShift == 0 && !p->initOffsets)
+            return sb_ctx_fail(c, SB_ERR_ARG, "pair %d: polyShift=0 needs initOffsets", k);
+        if (p->mask && (p->mask->nal <= 0 || p->mask->nrl <= 0 || !p->mask->mask))
+            return sb_ctx_fail(c, SB_ERR_ARG, "pair %d: invalid mask", k);
+        if (!out[k].offR || !out[k].offA || !out[k].corr || !out[k].type)
+            return sb_ctx_fail(c, SB_ERR_ARG, "pair %d: null output grid", k);
+        if (p->intf || (p->baseline && (p->baseline->Bn != 0 || p->baseline->Bp != 0 || p->baseline->dBn != 0 ||
+                                         p->baseline->dBp != 0 || p->baseline->dBnQ != 0 || p->baseline->dBpQ != 0)))
+            return sb_ctx_fail(c, SB_ERR_UNSUPPORTED, "pair %d: interferogram or baseline flattening: use sb_strack", k);
+        if (p->wR != p->wA || (p->maxTries > 0 && p->wRa != p->wAa))
+            return sb_ctx_fail(c, SB_ERR_UNSUPPORTED, "pair %d: windows must be square", k);
+        if (p->noComplex == 0 && !cmplx_supported(p->wR))
+            return sb_ctx_fail(c, SB_ERR_UNSUPPORTED, "pair %d: complex window %d not supported", k, p->wR);
+        if (p->maxTries > 0 && (!amp_supported(p->wRa) || (p->maxTries > 1 && !amp_supported(p->wRa * LA))))
+            return sb_ctx_fail(c, SB_ERR_UNSUPPORTED, "pair %d: amplitude window %d not supported", k, p->wRa);
+        if (p->noComplex != p0.noComplex || p->hanningFlag != p0.hanningFlag || p->maxTries != p0.maxTries ||
+            p->checkAzFocus != p0.checkAzFocus || p->gaussFlag != p0.gaussFlag ||
+            p->azDefocusThresh != p0.azDefocusThresh || p->scaleFactor != p0.scaleFactor)
+            return sb_ctx_fail(c, SB_ERR_ARG,
+                               "pair %d: the flags (noComplex, hanning, tries, checkAzFocus, gauss, azDefocusThresh, "
+                               "scaleFactor) must be the same for every pair of a batch", k);
+        total += (int64_t)p->nR * p->nA;
+    }
+    if (total > (int64_t)1 << 30) return sb_ctx_fail(c, SB_ERR_ARG, "batch grid too large");
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    cudaEventRecord(c->ev[0], c->stream);
+    for (int k = 0; k < 8; ++k) c->stage[k] = 0.f;
+
+    // ---- bucket order and atlases
+    std::vector<int> order(nPairs);
+    for (int k = 0; k < nPairs; ++k) order[k] = k;
+    std::stable_sort(order.begin(), order.end(), [P](int x, int y) {
+        return P[x].wR != P[y].wR ? P[x].wR < P[y].wR : P[x].wRa < P[y].wRa;
+    });
+    const size_t elem = I1[0].sampleType == SB_CFLOAT32 ? 8 : 4;
+    int width[2] = {0, 0};
+    std::vector<int64_t> rowOff[2] = {std::vector<int64_t>(nPairs), std::vector<int64_t>(nPairs)};
+    int64_t height[2] = {0, 0};
+    for (int q = 0; q < nPairs; ++q) {
+        const int k = order[q];
+        const sb_image* im[2] = {&I1[k], &I2[k]};
+        for (int i = 0; i < 2; ++i) {
+            width[i] = im[i]->nr > width[i] ? im[i]->nr : width[i];
+            rowOff[i][k] = height[i];
+            height[i] += im[i]->na;
+        }
+    }
+    if (height[0] >= ((int64_t)1 << 31) || height[1] >= ((int64_t)1 << 31))
+        return sb_ctx_fail(c, SB_ERR_ARG, "batch images too tall for one atlas");
+    cudaError_t e;
+    char* atlas[2];
+    for (int i = 0; i < 2; ++i) {
+        atlas[i] = (char*)sb_ctx_buf(c, i ? "atlas2" : "atlas1", (size_t)width[i] * height[i] * elem, &e);
+        if (!atlas[i]) return sb_ctx_cuda(c, e, "cudaMalloc(atlas)");
+    }
+    for (int k = 0; k < nPairs; ++k) {
+        const sb_image* im[2] = {&I1[k], &I2[k]};
+        for (int i = 0; i < 2; ++i) {
+            const size_t pitch = (size_t)width[i] * elem, rowB = (size_t)im[i]->nr * elem;
+            CK(cudaMemcpy2DAsync(atlas[i] + (size_t)rowOff[i][k] * pitch, pitch, im[i]->data, rowB, rowB,
+                                 (size_t)im[i]->na, im[i]->onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                 c->stream),
+               "atlas copy");
+        }
+    }
+    // ---- plans of every pair, offset into the atlases; complex lists per bucket
+    const int n = (int)total;
+    std::vector<PointPlan> plan((size_t)n);
+    std::vector<int> pairOf((size_t)n), clist, gStart(nPairs);
+    std::vector<Bucket> buckets;
+    {
+        std::vector<PointPlan> pl;
+        std::vector<int> cl;
+        int g = 0;
+        for (int q = 0; q < nPairs; ++q) {
+            const int k = order[q];
+            const sb_track_params* p = &P[k];
+            if (buckets.empty() || buckets.back().wR != p->wR || buckets.back().wRa != p->wRa) {
+                Bucket b;
+                b.wR = p->wR;
+                b.wRa = p->wRa;
+                b.pFirst = q;
+                b.g0 = g;
+                b.l0 = (int)clist.size();
+                buckets.push_back(b);
+            }
+            plan_strack(p, I1[k].nr, I1[k].na, I2[k].nr, I2[k].na, pl, cl);
+            gStart[k] = g;
+            for (size_t t = 0; t < pl.size(); ++t) {
+                PointPlan x = pl[t];
+                x.a1 += (int)rowOff[0][k];
+                x.a2 += (int)rowOff[1][k];
+                plan[(size_t)g + t] = x;
+                pairOf[(size_t)g + t] = k;
+            }
+            for (int v : cl) clist.push_back(g + v);
+            g += (int)pl.size();
+            buckets.back().pLast = q + 1;
+            buckets.back().g1 = g;
+            buckets.back().l1 = (int)clist.size();
+        }
+    }
+    PointPlan* dplan = (PointPlan*)sb_ctx_buf(c, "plan", sizeof(PointPlan) * n, &e);
+    PointRec* drec = (PointRec*)sb_ctx_buf(c, "rec", sizeof(PointRec) * n, &e);
+    int* dclist = (int*)sb_ctx_buf(c, "clist", sizeof(int) * (clist.size() + 1), &e);
+    int* dlist = (int*)sb_ctx_buf(c, "list", sizeof(int) * (n + 1), &e);
+    int* dpairOf = (int*)sb_ctx_buf(c, "pairOf", sizeof(int) * n, &e);
+    FitJob* dfit = (FitJob*)sb_ctx_buf(c, "fit", sizeof(FitJob) * (n + 1), &e);
+    unsigned long long* dstats = (unsigned long long*)sb_ctx_buf(c, "stats", sizeof(unsigned long long) * 8 * nPairs, &e);
+    float* dR = (float*)sb_ctx_buf(c, "offR", sizeof(float) * n, &e);
+    float* dA = (float*)sb_ctx_buf(c, "offA", sizeof(float) * n, &e);
+    float* dC = (float*)sb_ctx_buf(c, "corr", sizeof(float) * n, &e);
+    float* dZ = (float*)sb_ctx_buf(c, "azd", sizeof(float) * n, &e);
+    uint8_t* dT = (uint8_t*)sb_ctx_buf(c, "type", n, &e);
+    int* dkey = (int*)sb_ctx_buf(c, "listKey", sizeof(int) * (n + 1), &e);
+    int* dpart = (int*)sb_ctx_buf(c, "partScratch", sizeof(int) * partition_scratch_ints(n, PART_KMAX), &e);
+    int* dAz = (int*)sb_ctx_buf(c, "azEff", sizeof(int) * n, &e);
+    if (!dplan || !drec || !dclist || !dlist || !dpairOf || !dfit || !dstats || !dR || !dA || !dC || !dZ || !dT ||
+        !dkey || !dpart || !dAz)
+        return sb_ctx_fail(c, SB_ERR_NOMEM, "device allocation failed");
+    CK(cudaMemcpyAsync(dplan, plan.data(), sizeof(PointPlan) * n, cudaMemcpyHostToDevice, c->stream), "plan");
+    CK(cudaMemcpyAsync(dpairOf, pairOf.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c->stream), "pairOf");
+    if (!clist.empty())
+        CK(cudaMemcpyAsync(dclist, clist.data(), sizeof(int) * clist.size(), cudaMemcpyHostToDevice, c->stream),
+           "clist");
+    CK(cudaMemsetAsync(dstats, 0, sizeof(unsigned long long) * 8 * nPairs, c->stream), "memset");
+    cudaEventRecord(c->ev[1], c->stream);
+    CK(launch_rec_init(drec, n, c->stream), "rec_init");
+    c->launches++;
+
+    const int form = c->form;
+    int* dTcErr = (int*)sb_ctx_buf(c, "tcErr", sizeof(int), &e);
+    if (!dTcErr) return sb_ctx_fail(c, SB_ERR_NOMEM, "device allocation failed");
+    CK(cudaMemsetAsync(dTcErr, 0, sizeof(int), c->stream), "memset");
+    c->lastForm = SB_FORM_FP32;
+    constexpr int kPeakChunk = 1 << 19;
+    for (const Bucket& b : buckets) {
+        const sb_track_params* p = &P[order[b.pFirst]];  // windows and flags of the bucket
+        const int W = p->wR, WA = p->wRa;
+        const int nB = b.g1 - b.g0, nC = b.l1 - b.l0;
+        // ---- complex stage over the bucket's complex list
+        if (nC > 0) {
+            CmplxArgs a;
+            memset(&a, 0, sizeof(a));
+            a.img1 = atlas[0];
+            a.img2 = atlas[1];
+            a.nr1 = width[0]; a.na1 = (int)height[0]; a.nr2 = width[1]; a.na2 = (int)height[1];
+            a.sampleType = I1[0].sampleType;
+            a.byteOrder = I1[0].byteOrder;
+            a.plan = dplan;
+            a.nList = nC;
+            a.hanning = p->hanningFlag ? hanning_table(c, W) : nullptr;
+            a.hanCorr = p->hanningFlag ? 1.5 : 1.0;
+            a.twW = tw_table(c, W);
+            a.tau = tau_table(c, W);
+            a.osA = osA_table(c);
+            a.osD = osD_table(c);
+            a.gauss = p->gaussFlag ? 1 : 0;
+            a.azThresh = p->azDefocusThresh;
+            a.checkAzFocus = p->checkAzFocus;
+            a.noComplex = p->noComplex;
+            a.rec = drec;
+            if (!a.twW || !a.tau || !a.osA || !a.osD || (p->hanningFlag && !a.hanning))
+                return sb_ctx_fail(c, SB_ERR_NOMEM, "table allocation failed");
+            const bool tcForm = form == SB_FORM_SPLIT_BF16 && cmplx_tc_supported(W) && !p->gaussFlag && c->smMajor >= 10;
+            if (tcForm) {
+                a.tcErr = dTcErr;
+                c->lastForm = SB_FORM_SPLIT_BF16;
+            }
+            const int bpsm = tcForm ? cmplx_tc_blocks_per_sm() : cmplx_blocks_per_sm(W);
+            if (bpsm <= 0) return sb_ctx_fail(c, SB_ERR_CUDA, "complex kernel cannot be resident (W=%d)", W);
+            PeakJob* dpeak = nullptr;
+            if (!p->gaussFlag) {
+                const size_t pc = nC < kPeakChunk ? (size_t)nC : (size_t)kPeakChunk;
+                dpeak = (PeakJob*)sb_ctx_buf(c, "peakjob", pc * sizeof(PeakJob), &e);
+                if (!dpeak) return sb_ctx_fail(c, SB_ERR_NOMEM, "device allocation failed");
+            }
+            cudaEventRecord(c->sev[0], c->stream);
+            for (int off = 0; off < nC; off += kPeakChunk) {
+                const int cnt = nC - off < kPeakChunk ? nC - off : kPeakChunk;
+                CmplxArgs ak = a;
+                ak.list = dclist + b.l0 + off;
+                ak.fit = dfit + off;
+                ak.nList = cnt;
+                ak.peak = dpeak;
+                const int nCta = c->numSM * bpsm < cnt ? c->numSM * bpsm : cnt;
+                if (tcForm)
+                    CK(launch_strack_cmplx_tc(ak, nCta, c->stream), "strack_cmplx_tc");
+                else
+                    CK(launch_strack_cmplx(W, ak, nCta, c->stream), "strack_cmplx");
+                c->launches++;
+                if (dpeak) {
+                    PeakArgs pk;
+                    pk.peak = dpeak;
+                    pk.nList = cnt;
+                    pk.W = W;
+                    pk.hanCorr = a.hanCorr;
+                    pk.osD = a.osD;
+                    pk.rec = drec;
+                    pk.fit = dfit + off;
+                    CK(launch_strack_peak(pk, c->numSM, c->stream), "strack_peak");
+                    c->launches++;
+                }
+            }
+            FitArgs f = make_fit_args(p, dfit, nC, 0, drec);
+            CK(launch_strack_fit(f, c->stream), "strack_fit");
+            c->launches++;
+            cudaEventRecord(c->sev[1], c->stream);
+            CK(cudaEventSynchronize(c->sev[1]), "sync");
+            float t0 = 0;
+            cudaEventElapsedTime(&t0, c->sev[0], c->sev[1]);
+            c->stage[0] += t0;
+            c->stage[5] += (float)nC;
+        }
+        // ---- amplitude tries over the bucket's points
+        WalkParams w;
+        w.wR = p->wR; w.wA = p->wA; w.wRa = p->wRa; w.wAa = p->wAa;
+        w.noComplex = p->noComplex;
+        w.maxTries = p->maxTries;
+        const bool ownAz = (p->wRa == p->wR && p->wAa == p->wA);
+        PointPlan* bplan = dplan + b.g0;
+        PointRec* brec = drec + b.g0;
+        for (int stage = 1; stage <= 2 && stage <= p->maxTries; ++stage) {
+            CK(launch_select(bplan, brec, nB, w, stage, dkey, c->stream), "select");
+            CK(launch_partition(dkey, nullptr, nB, 1, dlist, dpart, c->stream), "partition");
+            c->launches += 4;
+            int cnt = 0;
+            CK(cudaMemcpyAsync(&cnt, dpart + partition_keyoff_at(nB, 1) + 1, sizeof(int), cudaMemcpyDeviceToHost,
+                               c->stream),
+               "count");
+            CK(cudaStreamSynchronize(c->stream), "sync");
+            if (cnt == 0) continue;
+            const int Ws = WA * (stage == 1 ? 1 : LA);
+            const bool needFill = !ownAz && !(p->noComplex && stage == 1);
+            if (needFill) {  // azShift carries over within a pair, from 0 at its first point
+                for (int q = b.pFirst; q < b.pLast; ++q) {
+                    const int k = order[q];
+                    CK(launch_az_fill(drec + gStart[k], P[k].nR * P[k].nA, dAz + (gStart[k] - b.g0), c->stream),
+                       "az_fill");
+                    c->launches++;
+                }
+            }
+            AmpArgs a;
+            memset(&a, 0, sizeof(a));
+            a.img1 = atlas[0];
+            a.img2 = atlas[1];
+            a.nr1 = width[0]; a.na1 = (int)height[0]; a.nr2 = width[1]; a.na2 = (int)height[1];
+            a.sampleType = I1[0].sampleType;
+            a.byteOrder = I1[0].byteOrder;
+            a.plan = bplan;
+            a.list = dlist;
+            a.nList = cnt;
+            a.stage = stage;
+            a.s = stage == 1 ? 1 : LA;
+            a.wR = p->wR; a.wA = p->wA; a.wRa = p->wRa; a.wAa = p->wAa;
+            a.noComplex = p->noComplex;
+            a.azThresh = p->azDefocusThresh;
+            a.checkAzFocus = p->checkAzFocus;
+            a.azEff = needFill ? dAz : nullptr;
+            a.twWs = tw_table(c, Ws);
+            a.tw2Ws = tw_table(c, 2 * Ws);
+            a.tau = tau_table(c, Ws);
+            a.osA = osA_table(c);
+            a.osD = osD_table(c);
+            a.gauss = p->gaussFlag ? 1 : 0;
+            a.rec = brec;
+            a.fit = dfit;
+            const bool onChip = amps_supported(Ws);
+            int nCta = c->numSM * (onChip ? amps_blocks_per_sm(Ws) : 2);
+            if (nCta > cnt) nCta = cnt;
+            if (nCta < 1) return sb_ctx_fail(c, SB_ERR_CUDA, "amplitude kernel cannot be resident (Ws=%d)", Ws);
+            if (!onChip) {
+                a.scratchPerCta = amp_scratch_elems(Ws);
+                a.scratch = (float2*)sb_ctx_buf(c, "ampScratch", sizeof(float2) * a.scratchPerCta * nCta, &e);
+            }
+            if ((!onChip && !a.scratch) || !a.twWs || !a.tw2Ws || !a.tau || !a.osA || !a.osD)
+                return sb_ctx_fail(c, SB_ERR_NOMEM, "amplitude workspace allocation failed");
+            if (onChip)
+                CK(launch_strack_amps(Ws, a, nCta, c->stream), "strack_amps");
+            else
+                CK(launch_strack_amp(Ws, a, nCta, c->stream), "strack_amp");
+            c->launches++;
+            FitArgs f = make_fit_args(p, dfit, cnt, stage, brec);
+            CK(launch_strack_fit(f, c->stream), "strack_fit");
+            c->launches++;
+            c->stage[5 + stage] += (float)cnt;
+        }
+        CK(launch_finalize(bplan, brec, nB, w, p->scaleFactor, dR + b.g0, dA + b.g0, dC + b.g0, dZ + b.g0, dT + b.g0,
+                           dstats, c->stream, dpairOf + b.g0),
+           "finalize");
+        c->launches++;
+    }
+    cudaEventRecord(c->ev[2], c->stream);
+    // ---- outputs, per pair
+    for (int k = 0; k < nPairs; ++k) {
+        const size_t g = (size_t)gStart[k], m = (size_t)P[k].nR * P[k].nA;
+        const int od = out[k].onDevice;
+        if ((rc = out_copy(c, out[k].offR, dR + g, sizeof(float) * m, od)) != SB_OK) return rc;
+        if ((rc = out_copy(c, out[k].offA, dA + g, sizeof(float) * m, od)) != SB_OK) return rc;
+        if ((rc = out_copy(c, out[k].corr, dC + g, sizeof(float) * m, od)) != SB_OK) return rc;
+        if (out[k].azd && (rc = out_copy(c, out[k].azd, dZ + g, sizeof(float) * m, od)) != SB_OK) return rc;
+        if ((rc = out_copy(c, out[k].type, dT + g, m, od)) != SB_OK) return rc;
+    }
+    std::vector<unsigned long long> st((size_t)8 * nPairs);
+    CK(cudaMemcpyAsync(st.data(), dstats, sizeof(unsigned long long) * 8 * nPairs, cudaMemcpyDeviceToHost, c->stream),
+       "stats");
+    int tcBad = 0;
+    CK(cudaMemcpyAsync(&tcBad, dTcErr, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "tcErr");
+    cudaEventRecord(c->ev[3], c->stream);
+    CK(cudaStreamSynchronize(c->stream), "strack_batch");
+    if (tcBad) return sb_ctx_fail(c, SB_ERR_TIMEOUT, "split-BF16 complex stage: a tensor-core wait timed out");
+    for (int k = 0; k < nPairs; ++k) {
+        const unsigned long long* s = &st[(size_t)8 * k];
+        out[k].nComplex = (int64_t)s[0];
+        out[k].nAmp = (int64_t)s[1];
+        out[k].nAmpL = (int64_t)s[2];
+        out[k].nFail = (int64_t)s[3];
+        out[k].nAttempted = (int64_t)P[k].nR * P[k].nA - (int64_t)s[4];
+    }
+    cudaEventElapsedTime(&c->timing[0], c->ev[0], c->ev[3]);
+    cudaEventElapsedTime(&c->timing[1], c->ev[0], c->ev[1]);
+    cudaEventElapsedTime(&c->timing[2], c->ev[1], c->ev[2]);
+    cudaEventElapsedTime(&c->timing[3], c->ev[2], c->ev[3]);
     return SB_OK;
 }

@@ -122,10 +122,10 @@ __global__ void __launch_bounds__(NT, (WS == 32 ? 3 : (WS == 48 ? 1 : 2))) strac
     for (int it = blockIdx.x; it < a.nList; it += gridDim.x) {
         const int p = a.list[it];
         const PointPlan pl = a.plan[p];
-        const int gi = p / a.nR, gj = p % a.nR;
-        // window corners (computeAmpImageLocations, speckleTrack.c:147-156)
-        const int a1a = a.aStart + gi * a.deltaA - a.wA / 2 * a.s;
-        const int r1a = a.rStart + gj * a.deltaR - a.wR / 2 * a.s;
+        // window corners (computeAmpImageLocations, speckleTrack.c:147-156):
+        // a1a = aStart + i deltaA - (wA/2) s = a1 + wA/2 - (wA/2) s, from the plan
+        const int a1a = pl.a1 + a.wA / 2 - a.wA / 2 * a.s;
+        const int r1a = pl.r1 + a.wR / 2 - a.wR / 2 * a.s;
         const int r2a = r1a + (pl.r2 - pl.r1);
         const int a2a = a1a + (pl.a2 - pl.a1);
         auto load = [&](float2* dst, int q) {

@@ -62,6 +62,7 @@ constexpr int MISC_BYTES = 3072;
 constexpr int SMEM_BYTES = OFF_MISC + MISC_BYTES + 1024;  // + alignment of the base to 1024
 constexpr int TMEM_COLS = 256;
 constexpr long long kWaitLimit = 1LL << 22;     // try_wait rounds per MMA completion
+constexpr long long kWaitCycles = 4000000000LL; // and at most ~2 s of SM clock cycles
 
 // ---------------------------------------------------------------- PTX helpers
 __device__ __forceinline__ uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -316,8 +317,9 @@ __global__ void __launch_bounds__(tcf::NT, 2) strack_cmplx_tc_kernel(CmplxArgs a
     auto wait_pass = [&]() -> bool {
         long long n = 0;
         bool ok = true;
+        const long long t0 = clock64();
         while (!mbar_try(bar, phase & 1u)) {
-            if (++n > kWaitLimit) {
+            if (++n > kWaitLimit || clock64() - t0 > kWaitCycles) {
                 ok = false;
                 break;
             }

@@ -67,10 +67,11 @@ __global__ void az_fill_kernel(const PointRec* rec, int n, int* azEff)
 
 __global__ void finalize_kernel(const PointPlan* plan, const PointRec* rec, int n, WalkParams w, int scaleFactor,
                                 float* offR, float* offA, float* corr, float* azd, uint8_t* type,
-                                unsigned long long* stats)
+                                unsigned long long* stats, const int* pairOf)
 {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
+    if (pairOf) stats += 8 * pairOf[p];  // batched calls: statistics per pair
     const PointPlan pl = plan[p];
     const PointRec r = rec[p];
     const WalkOut o = strack_walk(pl, r, w);
@@ -208,10 +209,11 @@ cudaError_t launch_az_fill(const PointRec* rec, int n, int* azEff, cudaStream_t 
 }
 cudaError_t launch_finalize(const PointPlan* plan, const PointRec* rec, int n, const WalkParams& w, int scaleFactor,
                             float* offR, float* offA, float* corr, float* azd, uint8_t* type,
-                            unsigned long long* stats, cudaStream_t st)
+                            unsigned long long* stats, cudaStream_t st, const int* pairOf)
 {
+    if (n <= 0) return cudaSuccess;
     finalize_kernel<<<(n + 255) / 256, 256, 0, st>>>(plan, rec, n, w, scaleFactor, offR, offA, corr, azd, type,
-                                                     stats);
+                                                     stats, pairOf);
     return cudaGetLastError();
 }
 

@@ -30,8 +30,9 @@ cudaError_t launch_band_key(const PointPlan* plan, const int* list, int n, int W
 cudaError_t launch_select(const PointPlan* plan, const PointRec* rec, int n, const WalkParams& w, int stage,
                           int* key, cudaStream_t st);
 cudaError_t launch_az_fill(const PointRec* rec, int n, int* azEff, cudaStream_t st);
+// pairOf (batched calls): pair of each point; statistics go to stats[8 * pair]
 cudaError_t launch_finalize(const PointPlan* plan, const PointRec* rec, int n, const WalkParams& w, int scaleFactor,
                             float* offR, float* offA, float* corr, float* azd, uint8_t* type,
-                            unsigned long long* stats, cudaStream_t st);
+                            unsigned long long* stats, cudaStream_t st, const int* pairOf = nullptr);
 
 }  // namespace sbk

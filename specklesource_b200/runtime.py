@@ -33,6 +33,8 @@ SIGNATURES = {
                             C.POINTER(abi.SbTrackResult)]),
     "sb_strackw": (C.c_int, [_P, C.POINTER(abi.SbTrackParams), C.POINTER(abi.SbImage), C.POINTER(abi.SbImage),
                              C.POINTER(abi.SbTrackResult)]),
+    "sb_strack_batch": (C.c_int, [_P, C.c_int32, C.POINTER(abi.SbTrackParams), C.POINTER(abi.SbImage),
+                                  C.POINTER(abi.SbImage), C.POINTER(abi.SbTrackResult)]),
     "sb_est_dop_carrier": (C.c_int, [_P, _P, _P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P]),
     "sb_cull": (C.c_int, [_P, C.POINTER(abi.SbCullParams), C.POINTER(abi.SbCullData)]),
     "sb_cull_st_data": (C.c_int, [_P, C.POINTER(abi.SbCullParams), C.POINTER(abi.SbCullData)]),
@@ -179,6 +181,31 @@ class Context:
     def strack(self, params, img1, img2, out=None):
         """speckleTrack (Strack/speckleTrack.c:159) on the GPU."""
         return self._track(self.lib.sb_strack, params, img1, img2, out, True)
+
+    def strack_batch(self, params, imgs1, imgs2):
+        """speckleTrack on many pairs in one call (sb_strack_batch): lists of
+        TrackParams and images; returns one result dict per pair."""
+        n = len(params)
+        if not (len(imgs1) == len(imgs2) == n) or n == 0:
+            raise ValueError("params, imgs1 and imgs2 must be non-empty lists of the same length")
+        keep, outs = [], []
+        P = (abi.SbTrackParams * n)()
+        I1 = (abi.SbImage * n)()
+        I2 = (abi.SbImage * n)()
+        R = (abi.SbTrackResult * n)()
+        for k in range(n):
+            pc, kp = params[k].to_c()
+            keep.append(kp)
+            P[k] = pc
+            I1[k] = image_desc(imgs1[k])
+            I2[k] = image_desc(imgs2[k])
+            o, r = abi.alloc_track_result(params[k].nA, params[k].nR, azd=True)
+            outs.append(o)
+            R[k] = r
+        self._check(self.lib.sb_strack_batch(self.h, n, P, I1, I2, R))
+        for k in range(n):
+            outs[k]["stats"] = abi.stats_of(R[k])
+        return outs
 
     def strackw(self, params, img1, img2, out=None):
         """corrTrackFast (Strackw/corrTrackFast.c:89) on the GPU."""

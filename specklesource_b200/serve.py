@@ -42,9 +42,10 @@ _AMP_SCRATCH = {16: 3 * 16 * 16 + 32 * 32 * 3 // 2, 24: 3 * 24 * 24 + 48 * 48 * 
 
 @dataclass
 class Job:
-    """One tracking job.  kind: "strack" or "strackw"; cull: CullParams or
-    None; inject: optional callable(offR, offA, corr, type) run on the host
-    copies of the offsets before culling (used to plant outliers)."""
+    """One tracking job.  kind: "strack", "strackw" or "cull" (culling only:
+    img1 = (offR, offA, corr, type)); cull: CullParams or None; inject:
+    optional callable(offR, offA, corr, type) run on the host copies of the
+    offsets before culling (used to plant outliers)."""
     kind: str
     params: Any
     img1: Any
@@ -67,6 +68,8 @@ def _image_bytes(img):
 
 def job_device_bytes(job, num_sm=148):
     """Upper estimate of the device memory a job holds while it runs."""
+    if job.kind == "cull":
+        return int(job.cull.nR) * int(job.cull.nA) * 64
     p = job.params
     n = int(p.nR) * int(p.nA)
     b = _image_bytes(job.img1) + _image_bytes(job.img2)
@@ -228,7 +231,13 @@ class JobServer:
 
 
 def run_job(ctx, job):
-    """Runs one job on a context (also how a job runs alone)."""
+    """Runs one job on a context (also how a job runs alone).  kind "cull":
+    culling only, job.img1 = (offR, offA, corr, type) grids."""
+    if job.kind == "cull":
+        offR, offA, corr, mt = (np.array(x, copy=True) for x in job.img1)
+        if job.inject is not None:
+            job.inject(offR, offA, corr, mt)
+        return {"track": None, "cull": ctx.cull(job.cull, offR, offA, corr, mt)}
     if job.kind == "strack":
         tr = ctx.strack(job.params, job.img1, job.img2)
     elif job.kind == "strackw":
