@@ -106,6 +106,24 @@ int sb_set_form(sb_context *ctx, int form);
 /* Form the complex stage of the last sb_strack call ran (SB_FORM_*). */
 int sb_last_form(const sb_context *ctx);
 
+/* Launch shape of one kernel for one window size, as an autotuner measured it
+ * (specklesource_b200/autotune.py writes the table the Python runtime
+ * applies).  No reference counterpart.  threads: a compiled thread count
+ * (0: the default); ctasPerSm: CTAs per SM of the persistent grid, at most
+ * the resident maximum (0: that maximum).  Kernels and windows:
+ *   SB_TUNE_COMPLEX     FP32 complex stage, window 16, 24, 32, 48 or 64
+ *   SB_TUNE_COMPLEX_TC  split-BF16 complex stage, window 64 (threads 0)
+ *   SB_TUNE_AMPLITUDE   shared-memory amplitude try, window 16, 24, 32 or 48
+ *                       (threads 0)
+ * Results do not depend on ctasPerSm; a different thread count changes the
+ * order of the float partial sums of the patch powers (not the transforms).
+ * Unknown kernels, windows or thread counts: SB_ERR_UNSUPPORTED; a CTA count
+ * above the resident maximum: SB_ERR_ARG. */
+#define SB_TUNE_COMPLEX 0
+#define SB_TUNE_COMPLEX_TC 1
+#define SB_TUNE_AMPLITUDE 2
+int sb_set_tuning(sb_context *ctx, int kernel, int window, int threads, int ctasPerSm);
+
 /* Device memory the context holds (bytes): the buffers its calls grew, kept
  * for reuse by later calls, and its constant tables.  No reference
  * counterpart (the reference mallocs per run and never frees). */

@@ -15,6 +15,9 @@ SB_ERR_NODEVICE = -5
 SB_ERR_TIMEOUT = -6
 SB_FORM_FP32 = 0
 SB_FORM_SPLIT_BF16 = 1
+SB_TUNE_COMPLEX = 0
+SB_TUNE_COMPLEX_TC = 1
+SB_TUNE_AMPLITUDE = 2
 
 SB_LARGEINT = 2000000000
 SB_BAD, SB_CMATCH, SB_AMPMATCH, SB_AMPMATCHLARGE = 0, 1, 2, 3

@@ -167,6 +167,79 @@ extern "C" int sb_set_form(sb_context* c, int form)
 
 extern "C" int sb_last_form(const sb_context* c) { return c ? c->lastForm : SB_FORM_FP32; }
 
+static int win_index(int W)
+{
+    switch (W) {
+    case 16: return 0;
+    case 24: return 1;
+    case 32: return 2;
+    case 48: return 3;
+    case 64: return 4;
+    default: return -1;
+    }
+}
+
+extern "C" int sb_set_tuning(sb_context* c, int kernel, int window, int threads, int ctasPerSm)
+{
+    if (!c) return SB_ERR_ARG;
+    c->err.clear();
+    if (ctasPerSm < 0) return sb_ctx_fail(c, SB_ERR_ARG, "ctasPerSm must be >= 0");
+    const int wi = win_index(window);
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) return sb_ctx_cuda(c, e, "cudaSetDevice");
+    if (kernel == SB_TUNE_COMPLEX) {
+        if (wi < 0) return sb_ctx_fail(c, SB_ERR_UNSUPPORTED, "complex window %d has no kernel", window);
+        if (threads != 0 && threads != cmplx_default_threads(window) && threads != cmplx_alt_threads(window))
+            return sb_ctx_fail(c, SB_ERR_UNSUPPORTED, "complex window %d: %d threads not compiled", window, threads);
+        const int mx = cmplx_blocks_per_sm(window, threads);
+        if (ctasPerSm > mx) return sb_ctx_fail(c, SB_ERR_ARG, "at most %d CTAs per SM at %d threads", mx, threads);
+        c->tuneCmplxThreads[wi] = threads;
+        c->tuneCmplxCtas[wi] = ctasPerSm;
+        return SB_OK;
+    }
+    if (kernel == SB_TUNE_COMPLEX_TC) {
+        if (!cmplx_tc_supported(window) || (threads != 0 && threads != 128))
+            return sb_ctx_fail(c, SB_ERR_UNSUPPORTED, "split-BF16 complex stage: window 64, 128 threads");
+        const int mx = cmplx_tc_blocks_per_sm();
+        if (ctasPerSm > mx) return sb_ctx_fail(c, SB_ERR_ARG, "at most %d CTAs per SM", mx);
+        c->tuneTcCtas = ctasPerSm;
+        return SB_OK;
+    }
+    if (kernel == SB_TUNE_AMPLITUDE) {
+        if (wi < 0 || !amps_supported(window) || threads != 0)
+            return sb_ctx_fail(c, SB_ERR_UNSUPPORTED, "shared-memory amplitude try: windows 16-48, default threads");
+        const int mx = amps_blocks_per_sm(window);
+        if (ctasPerSm > mx) return sb_ctx_fail(c, SB_ERR_ARG, "at most %d CTAs per SM", mx);
+        c->tuneAmpsCtas[wi] = ctasPerSm;
+        return SB_OK;
+    }
+    return sb_ctx_fail(c, SB_ERR_UNSUPPORTED, "unknown kernel %d", kernel);
+}
+
+// Launch shape of the complex stage at window W (tuning table or defaults).
+static void complex_shape(const sb_context* c, int W, bool tcForm, int* threads, int* bpsm)
+{
+    if (tcForm) {
+        *threads = 128;
+        const int mx = cmplx_tc_blocks_per_sm();
+        *bpsm = c->tuneTcCtas > 0 && c->tuneTcCtas < mx ? c->tuneTcCtas : mx;
+        return;
+    }
+    const int wi = win_index(W);
+    *threads = wi >= 0 ? c->tuneCmplxThreads[wi] : 0;
+    const int mx = cmplx_blocks_per_sm(W, *threads);
+    const int t = wi >= 0 ? c->tuneCmplxCtas[wi] : 0;
+    *bpsm = t > 0 && t < mx ? t : mx;
+}
+
+static int amps_ctas(const sb_context* c, int Ws)
+{
+    const int mx = amps_blocks_per_sm(Ws);
+    const int wi = win_index(Ws);
+    const int t = wi >= 0 ? c->tuneAmpsCtas[wi] : 0;
+    return t > 0 && t < mx ? t : mx;
+}
+
 extern "C" const char* sb_last_error(const sb_context* c)
 {
     if (!c) return "null context";
@@ -729,7 +802,8 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
             a.tcErr = dTcErr;
             tcErrFlag = dTcErr;
         }
-        int bpsm = tcForm ? cmplx_tc_blocks_per_sm() : cmplx_blocks_per_sm(W);
+        int cthreads = 0, bpsm = 0;
+        complex_shape(c, W, tcForm, &cthreads, &bpsm);
         if (bpsm <= 0) return sb_ctx_fail(c, SB_ERR_CUDA, "complex kernel cannot be resident (W=%d)", W);
         // per-band sub-lists (one band: the list as planned)
         std::vector<int> bandOff(bands.nb + 1, 0);
@@ -771,7 +845,7 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
                 if (tcForm)
                     CK(launch_strack_cmplx_tc(ak, nCta, c->stream), "strack_cmplx_tc");
                 else
-                    CK(launch_strack_cmplx(W, ak, nCta, c->stream), "strack_cmplx");
+                    CK(launch_strack_cmplx(W, ak, nCta, c->stream, cthreads), "strack_cmplx");
                 c->launches++;
                 if (dpeak) {
                     PeakArgs pk;
@@ -863,7 +937,7 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
         // small windows: everything in shared memory; larger: per-CTA
         // workspace in global memory staged through shared tiles
         const bool onChip = amps_supported(Ws);
-        int nCta = c->numSM * (onChip ? amps_blocks_per_sm(Ws) : 2);
+        int nCta = c->numSM * (onChip ? amps_ctas(c, Ws) : 2);
         if (nCta > cnt) nCta = cnt;
         if (nCta < 1) return sb_ctx_fail(c, SB_ERR_CUDA, "amplitude kernel cannot be resident (Ws=%d)", Ws);
         if (!onChip) {
@@ -1129,7 +1203,8 @@ extern "C" int sb_strack_batch(sb_context* c, int32_t nPairs, const sb_track_par
                 a.tcErr = dTcErr;
                 c->lastForm = SB_FORM_SPLIT_BF16;
             }
-            const int bpsm = tcForm ? cmplx_tc_blocks_per_sm() : cmplx_blocks_per_sm(W);
+            int cthreads = 0, bpsm = 0;
+            complex_shape(c, W, tcForm, &cthreads, &bpsm);
             if (bpsm <= 0) return sb_ctx_fail(c, SB_ERR_CUDA, "complex kernel cannot be resident (W=%d)", W);
             PeakJob* dpeak = nullptr;
             if (!p->gaussFlag) {
@@ -1149,7 +1224,7 @@ extern "C" int sb_strack_batch(sb_context* c, int32_t nPairs, const sb_track_par
                 if (tcForm)
                     CK(launch_strack_cmplx_tc(ak, nCta, c->stream), "strack_cmplx_tc");
                 else
-                    CK(launch_strack_cmplx(W, ak, nCta, c->stream), "strack_cmplx");
+                    CK(launch_strack_cmplx(W, ak, nCta, c->stream, cthreads), "strack_cmplx");
                 c->launches++;
                 if (dpeak) {
                     PeakArgs pk;
@@ -1228,7 +1303,7 @@ extern "C" int sb_strack_batch(sb_context* c, int32_t nPairs, const sb_track_par
             a.rec = brec;
             a.fit = dfit;
             const bool onChip = amps_supported(Ws);
-            int nCta = c->numSM * (onChip ? amps_blocks_per_sm(Ws) : 2);
+            int nCta = c->numSM * (onChip ? amps_ctas(c, Ws) : 2);
             if (nCta > cnt) nCta = cnt;
             if (nCta < 1) return sb_ctx_fail(c, SB_ERR_CUDA, "amplitude kernel cannot be resident (Ws=%d)", Ws);
             if (!onChip) {

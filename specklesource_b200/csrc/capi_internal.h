@@ -35,6 +35,12 @@ struct sb_context {
     cudaError_t noallocPrep = cudaSuccess;  // result of sb_noalloc_prepare at creation
     long long waitNaps = 1LL << 26;  // bounded device waits: 64 ns naps per wait (~4 s)
     int form = SB_FORM_FP32;         // transform form of the complex stage (sb_set_form)
+    // launch shapes set by sb_set_tuning (0: the library default); index by
+    // window: 16, 24, 32, 48, 64 -> 0..4
+    int tuneCmplxThreads[5] = {0, 0, 0, 0, 0};
+    int tuneCmplxCtas[5] = {0, 0, 0, 0, 0};
+    int tuneTcCtas = 0;
+    int tuneAmpsCtas[5] = {0, 0, 0, 0, 0};
     int lastForm = SB_FORM_FP32;     // form the last sb_strack call's complex stage ran
 };
 

@@ -574,28 +574,63 @@ static int occupancy_cmplx()
     return nb;
 }
 
+// Second thread count per window, for the autotuner (the default form's -gauss
+// instantiation keeps the default count).
+template <int W, int NT>
+static cudaError_t launch_cmplx_alt(const CmplxArgs& a, int nCta, cudaStream_t st)
+{
+    const bool f32 = a.sampleType == SB_CFLOAT32;
+    return f32 ? launch_cmplx_t<W, NT, true, false>(a, nCta, st) : launch_cmplx_t<W, NT, false, false>(a, nCta, st);
+}
+
 bool cmplx_supported(int W) { return W == 16 || W == 24 || W == 32 || W == 48 || W == 64; }
 
-int cmplx_blocks_per_sm(int W)
+int cmplx_default_threads(int W)
 {
     switch (W) {
-    case 16: return occupancy_cmplx<16, 64>();
-    case 24: return occupancy_cmplx<24, 96>();
-    case 32: return occupancy_cmplx<32, 256>();
-    case 48: return occupancy_cmplx<48, 192>();
-    case 64: return occupancy_cmplx<64, 256>();
+    case 16: return 64;
+    case 24: return 96;
+    case 32: return 256;
+    case 48: return 192;
+    case 64: return 256;
     default: return 0;
     }
 }
 
-cudaError_t launch_strack_cmplx(int W, const CmplxArgs& a, int nCta, cudaStream_t st)
+int cmplx_alt_threads(int W)
 {
     switch (W) {
-    case 16: return launch_cmplx<16, 64>(a, nCta, st);
-    case 24: return launch_cmplx<24, 96>(a, nCta, st);
-    case 32: return launch_cmplx<32, 256>(a, nCta, st);
-    case 48: return launch_cmplx<48, 192>(a, nCta, st);
-    case 64: return launch_cmplx<64, 256>(a, nCta, st);
+    case 16: return 128;
+    case 24: return 192;
+    case 32: return 128;
+    case 48: return 384;
+    case 64: return 512;
+    default: return 0;
+    }
+}
+
+int cmplx_blocks_per_sm(int W, int threads)
+{
+    const bool alt = threads != 0 && threads == cmplx_alt_threads(W);
+    switch (W) {
+    case 16: return alt ? occupancy_cmplx<16, 128>() : occupancy_cmplx<16, 64>();
+    case 24: return alt ? occupancy_cmplx<24, 192>() : occupancy_cmplx<24, 96>();
+    case 32: return alt ? occupancy_cmplx<32, 128>() : occupancy_cmplx<32, 256>();
+    case 48: return alt ? occupancy_cmplx<48, 384>() : occupancy_cmplx<48, 192>();
+    case 64: return alt ? occupancy_cmplx<64, 512>() : occupancy_cmplx<64, 256>();
+    default: return 0;
+    }
+}
+
+cudaError_t launch_strack_cmplx(int W, const CmplxArgs& a, int nCta, cudaStream_t st, int threads)
+{
+    const bool alt = threads != 0 && threads == cmplx_alt_threads(W) && !a.gauss;
+    switch (W) {
+    case 16: return alt ? launch_cmplx_alt<16, 128>(a, nCta, st) : launch_cmplx<16, 64>(a, nCta, st);
+    case 24: return alt ? launch_cmplx_alt<24, 192>(a, nCta, st) : launch_cmplx<24, 96>(a, nCta, st);
+    case 32: return alt ? launch_cmplx_alt<32, 128>(a, nCta, st) : launch_cmplx<32, 256>(a, nCta, st);
+    case 48: return alt ? launch_cmplx_alt<48, 384>(a, nCta, st) : launch_cmplx<48, 192>(a, nCta, st);
+    case 64: return alt ? launch_cmplx_alt<64, 512>(a, nCta, st) : launch_cmplx<64, 256>(a, nCta, st);
     default: return cudaErrorInvalidValue;
     }
 }

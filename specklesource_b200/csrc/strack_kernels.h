@@ -103,8 +103,12 @@ struct AmpArgs {
 };
 
 bool cmplx_supported(int W);
-int cmplx_blocks_per_sm(int W);
-cudaError_t launch_strack_cmplx(int W, const CmplxArgs& a, int nCta, cudaStream_t st);
+// thread counts compiled per window: the default and one alternative (0: none)
+int cmplx_default_threads(int W);
+int cmplx_alt_threads(int W);
+// resident CTAs per SM at `threads` (0: the default count)
+int cmplx_blocks_per_sm(int W, int threads = 0);
+cudaError_t launch_strack_cmplx(int W, const CmplxArgs& a, int nCta, cudaStream_t st, int threads = 0);
 
 // split-BF16 tensor-core form of the complex stage (strack_cmplx_tc.cu)
 bool cmplx_tc_supported(int W);

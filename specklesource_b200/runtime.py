@@ -27,6 +27,7 @@ SIGNATURES = {
     "sb_set_wait_limit": (C.c_int, [_P, C.c_int64]),
     "sb_set_form": (C.c_int, [_P, C.c_int]),
     "sb_context_device_bytes": (C.c_int64, [_P]),
+    "sb_set_tuning": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int]),
     "sb_context_release": (C.c_int, [_P]),
     "sb_last_form": (C.c_int, [_P]),
     "sb_strack": (C.c_int, [_P, C.POINTER(abi.SbTrackParams), C.POINTER(abi.SbImage), C.POINTER(abi.SbImage),
@@ -103,16 +104,33 @@ def image_desc(img, byte_order=None):
     return d
 
 
+def _device_name(device):
+    try:
+        import torch
+        return torch.cuda.get_device_name(device)
+    except Exception:
+        return None
+
+
 class Context:
     """One CUDA device, one stream; mirrors the reference's TrackParams/CullParams entry points."""
 
-    def __init__(self, device=0):
+    def __init__(self, device=0, tuning=None):
+        """tuning: None applies the autotuner's table (specklesource_b200/
+        tuning.json) when it was measured on a device of this name; False
+        applies none; a dict applies that table."""
         self.lib = load()
         h = C.c_void_p()
         rc = self.lib.sb_context_create(int(device), C.byref(h))
         if rc != abi.SB_OK:
             raise SpeckleError(rc, "sb_context_create failed (no CUDA device?)")
         self.h = h
+        self.tuning_applied = 0
+        if tuning is not False:
+            from . import autotune
+            table = tuning if isinstance(tuning, dict) else autotune.load()
+            if table and (isinstance(tuning, dict) or table.get("device") == _device_name(device)):
+                self.tuning_applied = autotune.apply(self, table)
 
     def close(self):
         if getattr(self, "h", None):
