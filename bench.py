@@ -648,7 +648,7 @@ def run_serving(args):
     torch.cuda.synchronize()
     gaps = rng.exponential(1.0 / 40.0, n_jobs)
     clocks = ClockSampler(0)
-    with serve.JobServer(slots=args.slots, hbm_budget=120e9) as srv:
+    with serve.JobServer(slots=args.slots, hbm_budget=120e9, max_batch=args.max_batch) as srv:
         # warm-up: the job set once, unpaced, so every slot's tables and
         # buffers exist (a long-running server's steady state)
         [f.result() for f in [srv.submit(j) for j, _ in jobs]]
@@ -670,7 +670,8 @@ def run_serving(args):
                         f"complex, W 32-64, {args.slots} slots, 120 GB budget", "jobs": n_jobs,
             "value": n_jobs / wall, "unit": "jobs/s", "patches_per_s": pts / wall,
             "latency_ms": serve.latency_stats(res), "offered_jobs_per_s": 40.0, "wall_s": wall,
-            "peak_admitted_gb": peak / 1e9, "clocks": clk}
+            "peak_admitted_gb": peak / 1e9, "max_batch": args.max_batch,
+            "batched_job_fraction": float(np.mean([r.get("batch", 1) > 1 for r in res])), "clocks": clk}
 
 
 def run_dftgemm(args):
@@ -855,6 +856,8 @@ def main():
     ap.add_argument("--no-other-form", action="store_true", help="skip measuring the other transform form")
     ap.add_argument("--slots", type=int, default=4, help="job-server slots for --workload cfg4/cfg5")
     ap.add_argument("--jobs", type=int, default=200, help="jobs offered in --workload cfg5")
+    ap.add_argument("--max-batch", type=int, default=8,
+                    help="job server: queued strack jobs that share one sb_strack_batch call (cfg5)")
     ap.add_argument("--batch", type=int, default=32768, help="patches per batch in --workload dftgemm")
     ap.add_argument("--workload", default="large", choices=["large", "small", "cfg1", "cfg3", "cfg3small", "cfg4", "cfg5", "cull", "dftgemm"],
                     help="small: 2400x4800 profiling case of the same generator; cfg1 / cfg3 / cull: the "

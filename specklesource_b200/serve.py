@@ -106,12 +106,14 @@ class JobServer:
     does not fit, idle slots release their buffers first.  Images passed as
     CUDA tensors belong to the caller and are not counted."""
 
-    def __init__(self, device=0, slots=4, hbm_budget=120e9, context_factory=None, num_sm=148):
+    def __init__(self, device=0, slots=4, hbm_budget=120e9, context_factory=None, num_sm=148, max_batch=1):
         if context_factory is None:
             from . import runtime
             context_factory = runtime.Context
         self.budget = float(hbm_budget)
         self.num_sm = num_sm
+        self.max_batch = int(max_batch)  # > 1: strack jobs queued together share one sb_strack_batch call
+        self.batches = []                # sizes of the batches run
         self._ctx = [context_factory(device) for _ in range(slots)]
         self._cv = threading.Condition()
         self._queue = collections.deque()
@@ -161,6 +163,8 @@ class JobServer:
         return fut
 
     def _take(self, k):
+        """Next work for slot k: a list of (job, need, future); more than one
+        when queued strack jobs can share one batched call."""
         ctx = self._ctx[k]
         with self._cv:
             while True:
@@ -170,11 +174,23 @@ class JobServer:
                     job, need, fut = self._queue[0]
                     if self._reserved(skip=k) + max(self._held[k], need) <= self.budget:
                         self._queue.popleft()
-                        self._running[k] = float(need)
+                        items = [(job, need, fut)]
+                        total = float(need)
+                        key = _batch_key(job)
+                        # continuous batching: later queued jobs that can share the call
+                        while (key is not None and len(items) < self.max_batch and self._queue and
+                               _batch_key(self._queue[0][0]) == key and
+                               self._reserved(skip=k) + max(self._held[k], total + self._queue[0][1]) <= self.budget):
+                            nxt = self._queue.popleft()
+                            items.append(nxt)
+                            total += nxt[1]
+                        self._running[k] = total
                         self._peak = max(self._peak, self._reserved())
-                        self.started.append((job.tag, time.perf_counter()))
+                        now = time.perf_counter()
+                        self.started += [(j.tag, now) for j, _, _ in items]
+                        self.batches.append(len(items))
                         self._cv.notify_all()
-                        return job, need, fut
+                        return items
                     if self._held[k] > 0 and getattr(ctx, "release", None):
                         # the head does not fit: this idle slot gives its buffers back
                         self._cv.release()
@@ -199,18 +215,24 @@ class JobServer:
     def _worker(self, k):
         ctx = self._ctx[k]
         while True:
-            item = self._take(k)
-            if item is None:
+            items = self._take(k)
+            if items is None:
                 return
-            job, need, fut = item
             try:
                 t0 = time.perf_counter()
-                res = run_job(ctx, job)
-                res.update(start=t0, end=time.perf_counter(), arrival=job.arrival, slot=k,
-                           held_bytes=self._measure(ctx))
-                fut.set_result(res)
-            except Exception as e:  # reported through the future
-                fut.set_exception(e)
+                if len(items) == 1:
+                    results = [run_job(ctx, items[0][0])]
+                else:
+                    results = run_batch(ctx, [j for j, _, _ in items])
+                t1 = time.perf_counter()
+                held = self._measure(ctx)
+                for (job, _, fut), res in zip(items, results):
+                    res.update(start=t0, end=t1, arrival=job.arrival, slot=k, held_bytes=held, batch=len(items))
+                    fut.set_result(res)
+            except Exception as e:  # reported through the futures
+                for _, _, fut in items:
+                    if not fut.done():
+                        fut.set_exception(e)
             finally:
                 self._finish(k)
 
@@ -254,6 +276,38 @@ def run_job(ctx, job):
             job.inject(offR, offA, corr, mt)
         cu = ctx.cull(job.cull, offR, offA, corr, mt)
     return {"track": tr, "cull": cu}
+
+
+def _batch_key(job):
+    """Jobs with equal keys can share one sb_strack_batch call (strack jobs
+    with the same flags and image sample type); None: the job runs alone."""
+    if job.kind != "strack" or not hasattr(job.params, "hanningFlag"):
+        return None
+    p = job.params
+    if getattr(p, "baseline", None) is not None or getattr(p, "intf", None) is not None:
+        return None
+    dt = getattr(job.img1, "dtype", None)
+    return (str(dt), p.noComplex, p.hanningFlag, p.maxTries, p.checkAzFocus, p.gaussFlag,
+            float(p.azDefocusThresh), p.scaleFactor)
+
+
+def run_batch(ctx, jobs):
+    """Runs strack jobs with one batched call (sb_strack_batch), then each
+    job's culling; per job the same result as run_job."""
+    tracks = ctx.strack_batch([j.params for j in jobs], [j.img1 for j in jobs], [j.img2 for j in jobs])
+    out = []
+    for job, tr in zip(jobs, tracks):
+        cu = None
+        if job.cull is not None:
+            offR = np.array(tr["offR"], np.float32, copy=True)
+            offA = np.array(tr["offA"], np.float32, copy=True)
+            corr = np.array(tr["corr"], np.float32, copy=True)
+            mt = np.array(tr["type"], np.uint8, copy=True)
+            if job.inject is not None:
+                job.inject(offR, offA, corr, mt)
+            cu = ctx.cull(job.cull, offR, offA, corr, mt)
+        out.append({"track": tr, "cull": cu})
+    return out
 
 
 def latency_stats(results):

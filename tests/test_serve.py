@@ -15,6 +15,7 @@ class FakeContext:
     lock = threading.Lock()
     running = 0
     max_running = 0
+    batch_calls = []
 
     def __init__(self, device):
         self.closed = False
@@ -36,6 +37,10 @@ class FakeContext:
 
     def strackw(self, p, a, b):
         return self._run(p)
+
+    def strack_batch(self, ps, a, b):
+        FakeContext.batch_calls.append(len(ps))
+        return [self._run(p) for p in ps]
 
     def cull(self, cp, offR, offA, corr, mt):
         return {"offRS": offR + 1}
@@ -126,6 +131,23 @@ def test_budget_counts_buffers_held_by_idle_slots():
     assert r["track"]["offR"][0, 0] == 200
 
 
+def test_queued_strack_jobs_share_a_batched_call():
+    """Continuous batching: jobs that queue while a slot is busy and can share
+    flags go into one strack_batch call; each future gets its own result, in
+    submission order; a job with other flags starts a new batch."""
+    FakeContext.running = FakeContext.max_running = 0
+    FakeContext.batch_calls = []
+    with serve.JobServer(slots=1, hbm_budget=1e12, context_factory=FakeContext, max_batch=4) as srv:
+        jobs = [_job(nR) for nR in (5, 6, 7, 8, 9, 10)]
+        jobs[4].params.hanningFlag = 0  # cannot join the others' batch
+        futs = [srv.submit(j) for j in jobs]
+        res = [f.result(timeout=10) for f in futs]
+    assert [r["track"]["offR"][0, 0] for r in res] == [5, 6, 7, 8, 9, 10]
+    assert max(srv.batches) > 1 and sum(srv.batches) == 6
+    assert FakeContext.batch_calls  # the batched entry point was used
+    assert [t for t, _ in srv.started] == [5, 6, 7, 8, 9, 10]
+
+
 def test_latency_stats():
     rs = [{"arrival": 0.0, "end": 0.001 * k} for k in range(1, 101)]
     st = serve.latency_stats(rs)
@@ -160,6 +182,15 @@ def test_same_result_alone_and_in_the_mix():
     with serve.JobServer(slots=3, hbm_budget=60e9) as srv:
         mixed = [f.result(timeout=600) for f in [srv.submit(j) for j in jobs]]
     assert len({r["slot"] for r in mixed}) > 1
+    # continuous batching: queued strack jobs share sb_strack_batch calls
+    with serve.JobServer(slots=1, hbm_budget=60e9, max_batch=4) as srv:
+        batched = [f.result(timeout=600) for f in [srv.submit(j) for j in jobs]]
+        assert max(srv.batches) > 1
+    for a, m in zip(alone, batched):
+        for k in ("offR", "offA", "corr", "type"):
+            assert np.array_equal(a["track"][k], m["track"][k], equal_nan=True), k
+        for k in ("offRS", "offAS", "type"):
+            assert np.array_equal(a["cull"][k], m["cull"][k], equal_nan=True), k
     for a, m in zip(alone, mixed):
         for k in ("offR", "offA", "corr", "type"):
             assert np.array_equal(a["track"][k], m["track"][k], equal_nan=True), k
