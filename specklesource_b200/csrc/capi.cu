@@ -198,8 +198,9 @@ extern "C" int sb_set_tuning(sb_context* c, int kernel, int window, int threads,
         return SB_OK;
     }
     if (kernel == SB_TUNE_COMPLEX_TC) {
-        if (!cmplx_tc_supported(window) || (threads != 0 && threads != 128))
-            return sb_ctx_fail(c, SB_ERR_UNSUPPORTED, "split-BF16 complex stage: window 64, 128 threads");
+        if (!cmplx_tc_supported(window) || (threads != 0 && threads != cmplx_tc_threads()))
+            return sb_ctx_fail(c, SB_ERR_UNSUPPORTED, "split-BF16 complex stage: window 64, %d threads",
+                               cmplx_tc_threads());
         const int mx = cmplx_tc_blocks_per_sm();
         if (ctasPerSm > mx) return sb_ctx_fail(c, SB_ERR_ARG, "at most %d CTAs per SM", mx);
         c->tuneTcCtas = ctasPerSm;
@@ -220,7 +221,7 @@ extern "C" int sb_set_tuning(sb_context* c, int kernel, int window, int threads,
 static void complex_shape(const sb_context* c, int W, bool tcForm, int* threads, int* bpsm)
 {
     if (tcForm) {
-        *threads = 128;
+        *threads = cmplx_tc_threads();
         const int mx = cmplx_tc_blocks_per_sm();
         *bpsm = c->tuneTcCtas > 0 && c->tuneTcCtas < mx ? c->tuneTcCtas : mx;
         return;

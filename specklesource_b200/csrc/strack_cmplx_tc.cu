@@ -36,11 +36,13 @@
 // conj(x))), with the conjugates folded into the cross spectrum (conj(S) =
 // conj(Z_1) Z_2) and the surface used as |c|^2 only.
 //
-// One CTA of 128 threads (4 warps) per patch, persistent over the list, two
-// CTAs per SM: 97 KB of shared memory (A operand 64 KB, DFT matrix 32 KB) and
-// 256 TMEM columns each (two 128-column accumulators).  Thread t owns TMEM
-// lane t, i.e. line t of every pass.  Waits on the MMA completion barrier are
-// bounded: on time-out the kernel records an error and returns.
+// One CTA of 256 threads (8 warps) per patch, persistent over the list, two
+// CTAs per SM: 100 KB of shared memory (A operand 64 KB, DFT matrix 32 KB) and
+// 256 TMEM columns each (two 128-column accumulators).  Two threads share each
+// TMEM lane L = line L of every pass: warps w and w + 4 read lanes
+// 32 (w mod 4) .. +31 and own the halves [0, 32) and [32, 64) of the line's
+// 64 values.  Waits on the MMA completion barrier are bounded: on time-out the
+// kernel records an error and returns.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -52,7 +54,7 @@ namespace sbk {
 namespace tcf {
 
 constexpr int W = 64;
-constexpr int NT = 128;
+constexpr int NT = 256;                         // two threads per TMEM lane
 constexpr int A_SUB = 128 * 128;                // bytes of one A sub-operand: 128 lines x 64 bf16
 constexpr int B_SUB = 64 * 128;                 // bytes of one B sub-operand: 64 rows x 64 bf16
 constexpr int OFF_A = 0;                        // Re hi | Re lo | Im hi | Im lo
@@ -119,21 +121,24 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar)
                  : "memory");
 }
 
-// 32 consecutive fp32 columns of this thread's TMEM lane
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32])
+// Two 32-column loads (the real and imaginary halves of an accumulator row)
+// and one wait, in one statement so nothing reads the registers before the wait.
+__device__ __forceinline__ void tmem_ld32x2(uint32_t ta, uint32_t tb, float (&va)[32], float (&vb)[32])
 {
-    uint32_t r[32];
+    uint32_t a[32], b[32];
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%64];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%65];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(a[0]), "=r"(a[1]), "=r"(a[2]), "=r"(a[3]), "=r"(a[4]), "=r"(a[5]), "=r"(a[6]), "=r"(a[7]), "=r"(a[8]), "=r"(a[9]), "=r"(a[10]), "=r"(a[11]), "=r"(a[12]), "=r"(a[13]), "=r"(a[14]), "=r"(a[15]), "=r"(a[16]), "=r"(a[17]), "=r"(a[18]), "=r"(a[19]), "=r"(a[20]), "=r"(a[21]), "=r"(a[22]), "=r"(a[23]), "=r"(a[24]), "=r"(a[25]), "=r"(a[26]), "=r"(a[27]), "=r"(a[28]), "=r"(a[29]), "=r"(a[30]), "=r"(a[31]),
+          "=r"(b[0]), "=r"(b[1]), "=r"(b[2]), "=r"(b[3]), "=r"(b[4]), "=r"(b[5]), "=r"(b[6]), "=r"(b[7]), "=r"(b[8]), "=r"(b[9]), "=r"(b[10]), "=r"(b[11]), "=r"(b[12]), "=r"(b[13]), "=r"(b[14]), "=r"(b[15]), "=r"(b[16]), "=r"(b[17]), "=r"(b[18]), "=r"(b[19]), "=r"(b[20]), "=r"(b[21]), "=r"(b[22]), "=r"(b[23]), "=r"(b[24]), "=r"(b[25]), "=r"(b[26]), "=r"(b[27]), "=r"(b[28]), "=r"(b[29]), "=r"(b[30]), "=r"(b[31])
+        : "r"(ta), "r"(tb)
+        : "memory");
 #pragma unroll
-    for (int k = 0; k < 32; ++k) v[k] = __uint_as_float(r[k]);
+    for (int k = 0; k < 32; ++k) {
+        va[k] = __uint_as_float(a[k]);
+        vb[k] = __uint_as_float(b[k]);
+    }
 }
 
 // ---------------------------------------------------------------- operand layout
@@ -264,11 +269,15 @@ __global__ void __launch_bounds__(tcf::NT, 2) strack_cmplx_tc_kernel(CmplxArgs a
     uint64_t* bar = reinterpret_cast<uint64_t*>(misc);                  // 8 B
     uint32_t* tslot = reinterpret_cast<uint32_t*>(misc + 8);            // 4 B
     int* azs = reinterpret_cast<int*>(misc + 12);                       // 4 B
-    double* red = reinterpret_cast<double*>(misc + 16);                 // (4 + 1) x 19 doubles = 760 B
-    float2* tau = reinterpret_cast<float2*>(misc + 1024);               // 64 x 8 B = 512 B
-    unsigned* iscr = reinterpret_cast<unsigned*>(misc + 1536);          // 8 words
-    unsigned long long* lowm = reinterpret_cast<unsigned long long*>(misc + 2048);  // 128 row masks
-    const int tid = threadIdx.x, warp = tid >> 5;
+    double* red = reinterpret_cast<double*>(misc + 16);                 // (8 + 1) x 19 doubles = 1368 B
+    float2* tau = reinterpret_cast<float2*>(misc + 1408);               // 64 x 8 B
+    unsigned* iscr = reinterpret_cast<unsigned*>(misc + 1920);          // 16 words
+    uint32_t* lowm = reinterpret_cast<uint32_t*>(misc + 2048);          // 128 lines x 2 halves
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    // two threads per TMEM lane: warps 0-3 and 4-7 cover lanes 0-127 twice;
+    // thread (L, h) owns line L and the half h of its 64 values
+    const int L = ((warp & 3) << 5) | lane, h = warp >> 2;
+    const int w = L >> 6, k = L & 63;
     const uint32_t aBase = su32(A), bBase = su32(Bm);
 
     // ---- DFT matrix F[t][n] = exp(-2 pi i t n / 64) as hi/lo bf16, K-major rows n
@@ -308,7 +317,7 @@ __global__ void __launch_bounds__(tcf::NT, 2) strack_cmplx_tc_kernel(CmplxArgs a
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tslot;
-    const uint32_t tlane = tmem + ((uint32_t)(warp * 32) << 16);  // this warp's lane quarter
+    const uint32_t tlane = tmem + ((uint32_t)((warp & 3) * 32) << 16);  // this warp's lane quarter
     uint32_t phase = 0;
     bool failed = false;
 
@@ -338,42 +347,61 @@ __global__ void __launch_bounds__(tcf::NT, 2) strack_cmplx_tc_kernel(CmplxArgs a
             issue_pass(aBase, bBase, aMN, tmem, dcol, bar);
         }
     };
+    // the half h of a 128-column accumulator (Re at dcol, Im at dcol + 64) into
+    // chunks 4h .. 4h+3 of an A row
+    auto drain_half = [&](uint32_t dcol, uint32_t rowOff, int swz) {
+        float vr[32], vi[32];
+        tmem_ld32x2(tlane + dcol + 32 * h, tlane + dcol + 64 + 32 * h, vr, vi);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            float re[8], im[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                re[q] = vr[8 * c + q];
+                im[q] = vi[8 * c + q];
+            }
+            put_chunk(A, rowOff, swz, 4 * h + c, re, im);
+        }
+    };
 
     const float thr = F32 ? 1e-15f : 1e-9f;
     const float thrAll = thr * W * W;
-    const int w = tid >> 6, k = tid & 63;  // load phase: window w, range column k
 
     for (int it = blockIdx.x; it < a.nList && !failed; it += gridDim.x) {
         const int p = a.list[it];
         const PointPlan pl = a.plan[p];
-        // ------------------------------------------------ getPatches: column k of window w
+        // ------------------------------------------------ getPatches: column k of window w, rows [32 h, 32 h + 32)
         // power / mean sums in float per thread, totals in double; lag-1 sums
         // along azimuth in double (mean-corrected after the reduction)
         const void* img = w ? a.img2 : a.img1;
         const int nr = w ? a.nr2 : a.nr1;
         const int r0 = (w ? pl.a2 : pl.a1), c0 = (w ? pl.r2 : pl.r1) + k;
+        auto sample = [&](int i) {
+            float2 v = tc_sample<F32>(img, nr, r0 + i, c0, a.byteOrder);
+            if (w && a.hanning) {
+                const float hv = __ldg(a.hanning + i * W + k);
+                v.x *= hv;
+                v.y *= hv;
+            }
+            return v;
+        };
         float fp = 0.f, fr = 0.f, fi = 0.f;
-        unsigned long long low = 0;  // rows whose power is below the threshold
-        double lr = 0, li = 0, nr_ = 0, ni_ = 0, pr_ = 0, pi_ = 0;  // sum z[i+1] conj z[i], sum z[1..], sum z[..62]
-        float2 prev = make_float2(0.f, 0.f);
-        const uint32_t rowOff = row_kmajor(tid);
+        uint32_t low = 0;  // rows of this half whose power is below the threshold
+        double lr = 0, li = 0, nr_ = 0, ni_ = 0, pr_ = 0, pi_ = 0;  // sum z[i] conj z[i-1], sum z[1..], sum z[..62]
+        float2 prev = h ? sample(31) : make_float2(0.f, 0.f);      // the pair (31, 32) belongs to half 1
+        const uint32_t rowOff = row_kmajor(L);
 #pragma unroll 1
-        for (int g = 0; g < 8; ++g) {  // 8 rows per chunk of the K-major F1 operand
+        for (int g = 0; g < 4; ++g) {  // 8 rows per chunk of the K-major F1 operand
             float2 z[8];
 #pragma unroll
-            for (int q = 0; q < 8; ++q) z[q] = tc_sample<F32>(img, nr, r0 + 8 * g + q, c0, a.byteOrder);
+            for (int q = 0; q < 8; ++q) z[q] = sample(32 * h + 8 * g + q);
             float re[8], im[8];
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
-                const int i = 8 * g + q;
-                float2 v = z[q];
-                if (w && a.hanning) {
-                    const float h = __ldg(a.hanning + i * W + k);
-                    v.x *= h;
-                    v.y *= h;
-                }
+                const int i = 32 * h + 8 * g + q;
+                const float2 v = z[q];
                 const float pw = __fadd_rn(__fmul_rn(v.x, v.x), __fmul_rn(v.y, v.y));
-                low |= (unsigned long long)(pw < thr) << i;
+                low |= (uint32_t)(pw < thr) << (8 * g + q);
                 fp += pw;
                 fr += v.x;
                 fi += v.y;
@@ -391,12 +419,12 @@ __global__ void __launch_bounds__(tcf::NT, 2) strack_cmplx_tc_kernel(CmplxArgs a
                 re[q] = v.x;
                 im[q] = v.y;
             }
-            put_chunk(A, rowOff, tid & 7, g, re, im);
+            put_chunk(A, rowOff, L & 7, 4 * h + g, re, im);
         }
         // getPatches counts the positions where either window's power is low
-        lowm[tid] = low;
+        lowm[2 * L + h] = low;
         __syncthreads();
-        const int nLow = w ? 0 : __popcll(lowm[tid] | lowm[tid + 64]);
+        const int nLow = w ? 0 : __popc(lowm[2 * L + h] | lowm[2 * (L + 64) + h]);
         // block totals: [0..1] power, [2..5] sums (re, im) of windows 1, 2,
         // [6] low positions, [7..18] lag, next, prev sums of windows 1, 2
         double s[19];
@@ -447,63 +475,40 @@ __global__ void __launch_bounds__(tcf::NT, 2) strack_cmplx_tc_kernel(CmplxArgs a
         // ------------------------------------------------ F1: azimuth transforms of both windows
         run_pass(false, 0);
         if (!wait_pass()) { failed = true; break; }
-        // ------------------------------------------------ F2: range transforms (D1 -> MN-major A)
-        {
-            const uint32_t ro = row_mnmajor(k, w);
-#pragma unroll 1
-            for (int h = 0; h < 2; ++h) {
-                float vr[32], vi[32];
-                tmem_ld32(tlane + 0 + 32 * h, vr);
-                tmem_ld32(tlane + 64 + 32 * h, vi);
-#pragma unroll
-                for (int c = 0; c < 4; ++c) {
-                    float re[8], im[8];
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) {
-                        re[q] = vr[8 * c + q];
-                        im[q] = vi[8 * c + q];
-                    }
-                    put_chunk(A, ro, k & 7, 4 * h + c, re, im);
-                }
-            }
-        }
+        // ------------------------------------------------ F2: range transforms (D1 -> MN-major A, K row k of atom w)
+        drain_half(0, row_mnmajor(k, w), k & 7);
         run_pass(true, 128);
         if (!wait_pass()) { failed = true; break; }
         // ------------------------------------------------ cross spectrum, conjugated: conj(Z1) Z2
-        // thread (w, n1) holds Z_w[n1][.]; it computes columns [32 w, 32 w + 32)
-        // and receives the other window's half of its row through shared memory
-        float2 S[32];
+        // thread (w, n1, h) holds Z_w[n1][32 h .. 32 h + 31]; it computes the
+        // 16 columns 32 h + 16 w + j and takes the other window's 16 values
+        // from its partner (line L ^ 64, same half) through shared memory
+        float2 S[16];
         {
-            float2* xb = reinterpret_cast<float2*>(A);  // 32 x 128 float2: [j][thread]
-            const int other = tid ^ 64;
-            {
-                float vr[32], vi[32];
-                const int hx = 1 - w;  // the half the partner needs
-                tmem_ld32(tlane + 128 + 32 * hx, vr);
-                tmem_ld32(tlane + 192 + 32 * hx, vi);
-                tc_fence_before();
-                __syncthreads();  // F2's operand reads are complete (waited), the area is free
-#pragma unroll
-                for (int j = 0; j < 32; ++j) xb[j * NT + tid] = make_float2(vr[j], vi[j]);
-            }
             float vr[32], vi[32];
-            tmem_ld32(tlane + 128 + 32 * w, vr);
-            tmem_ld32(tlane + 192 + 32 * w, vi);
+            tmem_ld32x2(tlane + 128 + 32 * h, tlane + 192 + 32 * h, vr, vi);
+            float2* xb = reinterpret_cast<float2*>(A);  // 16 x 256 float2: [j][thread]
+            tc_fence_before();
+            __syncthreads();  // F2's operand reads are complete (waited): the area is free
+            // compile-time register indices, selected by the window (no local array)
+#pragma unroll
+            for (int j = 0; j < 16; ++j)  // the columns the partner computes
+                xb[j * NT + tid] = w ? make_float2(vr[j], vi[j]) : make_float2(vr[16 + j], vi[16 + j]);
             __syncthreads();
 #pragma unroll
-            for (int j = 0; j < 32; ++j) {
-                const float2 o = xb[j * NT + other];
-                const float2 z1 = w ? o : make_float2(vr[j], vi[j]);
-                const float2 z2 = w ? make_float2(vr[j], vi[j]) : o;
-                // conj(z1) z2
-                S[j] = make_float2(z1.x * z2.x + z1.y * z2.y, z1.x * z2.y - z1.y * z2.x);
+            for (int j = 0; j < 16; ++j) {
+                const float2 o = xb[j * NT + (tid ^ 64)];
+                const float2 own = w ? make_float2(vr[16 + j], vi[16 + j]) : make_float2(vr[j], vi[j]);
+                const float2 z1 = w ? o : own;
+                const float2 z2 = w ? own : o;
+                S[j] = make_float2(z1.x * z2.x + z1.y * z2.y, z1.x * z2.y - z1.y * z2.x);  // conj(z1) z2
             }
             tc_fence_before();
             __syncthreads();  // everyone has read xb before the area becomes the A operand
         }
         const int az = *azs;
-        const int n1 = k;
-        const int krow = (n1 - az) & 63;  // K row k1' = n1 - azShift (mod 64) holds S row n1
+        const int krow = (k - az) & 63;  // K row k1' = n1 - azShift (mod 64) holds S row n1 = k
+        const int k2base = 32 * h + 16 * w;
         // ------------------------------------------------ I1_e1: inverse along k1 (two parities)
 #pragma unroll 1
         for (int e1 = 0; e1 < 2; ++e1) {
@@ -513,21 +518,21 @@ __global__ void __launch_bounds__(tcf::NT, 2) strack_cmplx_tc_kernel(CmplxArgs a
             for (int e2 = 0; e2 < 2; ++e2) {
                 const uint32_t ro = row_mnmajor(krow, e2);
 #pragma unroll
-                for (int c = 0; c < 4; ++c) {
+                for (int c = 0; c < 2; ++c) {
                     float re[8], im[8];
 #pragma unroll
                     for (int q = 0; q < 8; ++q) {
-                        const int j = 8 * c + q, k2 = 32 * w + j;
+                        const int j = 8 * c + q;
                         float2 v = S[j];
                         v = make_float2(v.x * tr.x - v.y * tr.y, v.x * tr.y + v.y * tr.x);
                         if (e2) {
-                            const float2 t2 = make_float2(tau[k2].x, -tau[k2].y);
+                            const float2 t2 = make_float2(tau[k2base + j].x, -tau[k2base + j].y);
                             v = make_float2(v.x * t2.x - v.y * t2.y, v.x * t2.y + v.y * t2.x);
                         }
                         re[q] = v.x;
                         im[q] = v.y;
                     }
-                    put_chunk(A, ro, krow & 7, 4 * w + c, re, im);
+                    put_chunk(A, ro, krow & 7, (k2base >> 3) + c, re, im);
                 }
             }
             run_pass(true, e1 ? 128 : 0);
@@ -535,86 +540,80 @@ __global__ void __launch_bounds__(tcf::NT, 2) strack_cmplx_tc_kernel(CmplxArgs a
         }
         if (failed) break;
         // ------------------------------------------------ I2_e1: inverse along k2
-        // thread (e2, k2) holds D3_e1[(e2,k2)][m1]: K row k2 of M atom e2
-        float pmax = 0.f;
+        // thread (e2, k2, h) holds D3_e1[(e2,k2)][m1] for m1 in half h: K row k2 of M atom e2
 #pragma unroll 1
         for (int e1 = 0; e1 < 2; ++e1) {
             const uint32_t dcol = e1 ? 128u : 0u;
-            const uint32_t ro = row_mnmajor(k, w);
-#pragma unroll 1
-            for (int h = 0; h < 2; ++h) {
-                float vr[32], vi[32];
-                tmem_ld32(tlane + dcol + 32 * h, vr);
-                tmem_ld32(tlane + dcol + 64 + 32 * h, vi);
-#pragma unroll
-                for (int c = 0; c < 4; ++c) {
-                    float re[8], im[8];
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) {
-                        re[q] = vr[8 * c + q];
-                        im[q] = vi[8 * c + q];
-                    }
-                    put_chunk(A, ro, k & 7, 4 * h + c, re, im);
-                }
-            }
+            drain_half(dcol, row_mnmajor(k, w), k & 7);
             run_pass(true, dcol);
             if (!wait_pass()) { failed = true; break; }
         }
         if (failed) break;
-        // ------------------------------------------------ |c|^2 planes (thread (e2, m1) owns row m1 of (e1, e2))
+        // ------------------------------------------------ |c|^2 planes (thread (e2, m1, h): row m1, half h of (e1, e2))
         float* P = reinterpret_cast<float*>(A);
+        float pmax = 0.f;
         {
             const int e2 = w, m1 = k;
 #pragma unroll 1
             for (int e1 = 0; e1 < 2; ++e1) {
                 const int q = 2 * e1 + e2;
-#pragma unroll 1
-                for (int h = 0; h < 2; ++h) {
-                    float vr[32], vi[32];
-                    tmem_ld32(tlane + (e1 ? 128u : 0u) + 32 * h, vr);
-                    tmem_ld32(tlane + (e1 ? 128u : 0u) + 64 + 32 * h, vi);
+                float vr[32], vi[32];
+                tmem_ld32x2(tlane + (e1 ? 128u : 0u) + 32 * h, tlane + (e1 ? 128u : 0u) + 64 + 32 * h, vr, vi);
 #pragma unroll
-                    for (int c4 = 0; c4 < 8; ++c4) {
-                        float4 o;
-                        o.x = vr[4 * c4 + 0] * vr[4 * c4 + 0] + vi[4 * c4 + 0] * vi[4 * c4 + 0];
-                        o.y = vr[4 * c4 + 1] * vr[4 * c4 + 1] + vi[4 * c4 + 1] * vi[4 * c4 + 1];
-                        o.z = vr[4 * c4 + 2] * vr[4 * c4 + 2] + vi[4 * c4 + 2] * vi[4 * c4 + 2];
-                        o.w = vr[4 * c4 + 3] * vr[4 * c4 + 3] + vi[4 * c4 + 3] * vi[4 * c4 + 3];
-                        pmax = fmaxf(pmax, fmaxf(fmaxf(o.x, o.y), fmaxf(o.z, o.w)));
-                        const int m2 = 32 * h + 4 * c4;
-                        *reinterpret_cast<float4*>(P + pidx(q, m1, m2)) = o;
-                    }
+                for (int c4 = 0; c4 < 8; ++c4) {
+                    float4 o;
+                    o.x = vr[4 * c4 + 0] * vr[4 * c4 + 0] + vi[4 * c4 + 0] * vi[4 * c4 + 0];
+                    o.y = vr[4 * c4 + 1] * vr[4 * c4 + 1] + vi[4 * c4 + 1] * vi[4 * c4 + 1];
+                    o.z = vr[4 * c4 + 2] * vr[4 * c4 + 2] + vi[4 * c4 + 2] * vi[4 * c4 + 2];
+                    o.w = vr[4 * c4 + 3] * vr[4 * c4 + 3] + vi[4 * c4 + 3] * vi[4 * c4 + 3];
+                    pmax = fmaxf(pmax, fmaxf(fmaxf(o.x, o.y), fmaxf(o.z, o.w)));
+                    *reinterpret_cast<float4*>(P + pidx(q, m1, 32 * h + 4 * c4)) = o;
                 }
             }
         }
-        tc_fence_before();
-        __syncthreads();
         // ------------------------------------------------ findCPeak (exact tie order, as strack_cmplx.cu)
+        // the block maximum of |c|^2, then every value whose sqrtf equals its
+        // sqrtf is ranked in findCPeak's scan order; each thread rescans the
+        // 64 values it wrote
         int iMax = 0, jMax = 0;
         {
-            const int lane = tid & 31;
             unsigned u = __reduce_max_sync(0xffffffffu, __float_as_uint(pmax));
             if (lane == 0) iscr[warp] = u;
+            tc_fence_before();
             __syncthreads();
-            u = max(max(iscr[0], iscr[1]), max(iscr[2], iscr[3]));
+            u = iscr[0];
+#pragma unroll
+            for (int q = 1; q < NT / 32; ++q) u = max(u, iscr[q]);
             const float pm = __uint_as_float(u);
             if (pm > 0.f) {  // uniform
                 const float smx = sqrtf(pm);
                 const float lo = pm * (1.0f - 1.0f / 1048576.0f);
                 unsigned best = 0xffffffffu;
-                for (int e = tid; e < 4 * 4096; e += NT) {
-                    const int q = e >> 12, m1 = (e >> 6) & 63, m2 = e & 63;
-                    const float v = P[pidx(q, m1, m2)];
-                    if (v >= lo && sqrtf(v) == smx) {
-                        const int cy = 2 * m1 + (q >> 1), cx = 2 * m2 + (q & 1);
-                        const int y = cy < W ? cy + W : cy - W, x = cx < W ? cx + W : cx - W;
-                        best = min(best, (unsigned)cpeak_rank(y, x, W));
+                const int e2 = w, m1 = k;
+#pragma unroll 1
+                for (int e1 = 0; e1 < 2; ++e1) {
+                    const int q = 2 * e1 + e2;
+#pragma unroll
+                    for (int c4 = 0; c4 < 8; ++c4) {
+                        const int m2b = 32 * h + 4 * c4;
+                        const float4 v4 = *reinterpret_cast<const float4*>(P + pidx(q, m1, m2b));
+                        const float vv[4] = {v4.x, v4.y, v4.z, v4.w};
+#pragma unroll
+                        for (int t = 0; t < 4; ++t) {
+                            if (vv[t] >= lo && sqrtf(vv[t]) == smx) {
+                                const int cy = 2 * m1 + e1, cx = 2 * (m2b + t) + e2;
+                                const int y = cy < W ? cy + W : cy - W, x = cx < W ? cx + W : cx - W;
+                                best = min(best, (unsigned)cpeak_rank(y, x, W));
+                            }
+                        }
                     }
                 }
                 best = __reduce_min_sync(0xffffffffu, best);
-                if (lane == 0) iscr[4 + warp] = best;
+                if (lane == 0) iscr[NT / 32 + warp] = best;
                 __syncthreads();
-                best = min(min(iscr[4], iscr[5]), min(iscr[6], iscr[7]));
+                best = iscr[NT / 32];
+#pragma unroll
+                for (int q = 1; q < NT / 32; ++q) best = min(best, iscr[NT / 32 + q]);
                 const int qq = best & 3, ij = best >> 2;
                 iMax = ij / W + ((qq == 1 || qq == 2) ? W : 0);
                 jMax = ij % W + ((qq == 1 || qq == 3) ? W : 0);
@@ -683,17 +682,37 @@ static cudaError_t launch_tc_t(const CmplxArgs& a, int nCta, cudaStream_t st)
     cudaError_t e = cudaFuncSetAttribute(strack_cmplx_tc_kernel<F32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          SMEM_BYTES);
     if (e != cudaSuccess) return e;
+    // the largest shared-memory carveout, so that two CTAs fit on an SM
+    e = cudaFuncSetAttribute(strack_cmplx_tc_kernel<F32>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return e;
     strack_cmplx_tc_kernel<F32><<<nCta, NT, SMEM_BYTES, st>>>(a);
     return cudaGetLastError();
 }
 
 bool cmplx_tc_supported(int W_) { return W_ == tcf::W; }
 
+int cmplx_tc_threads() { return NT; }
+
+// Resident CTAs per SM from the SM's register file, shared memory and thread
+// slots and the kernel's attributes.  (On the B200 the runtime's occupancy
+// calculator reports one CTA for this kernel where the launch statistics show
+// two resident; the resources are counted here instead.)
 int cmplx_tc_blocks_per_sm()
 {
-    int nb = 0;
-    cudaFuncSetAttribute(strack_cmplx_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, strack_cmplx_tc_kernel<true>, NT, SMEM_BYTES);
+    int dev = 0;
+    cudaDeviceProp pr;
+    cudaFuncAttributes fa;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&pr, dev) != cudaSuccess ||
+        cudaFuncGetAttributes(&fa, strack_cmplx_tc_kernel<true>) != cudaSuccess)
+        return 0;
+    const int regsPerWarp = ((fa.numRegs * 32 + 255) / 256) * 256;  // allocation unit of 256 registers per warp
+    const int byRegs = pr.regsPerMultiprocessor / (regsPerWarp * (NT / 32));
+    const size_t perCta = (size_t)SMEM_BYTES + fa.sharedSizeBytes + pr.reservedSharedMemPerBlock;
+    const int bySmem = (int)(pr.sharedMemPerMultiprocessor / perCta);
+    const int byThreads = pr.maxThreadsPerMultiProcessor / NT;
+    int nb = byRegs < bySmem ? byRegs : bySmem;
+    nb = nb < byThreads ? nb : byThreads;
     // two 256-column TMEM allocations fill an SM's 512 columns: never more
     return nb > 2 ? 2 : nb;
 }

@@ -112,6 +112,7 @@ cudaError_t launch_strack_cmplx(int W, const CmplxArgs& a, int nCta, cudaStream_
 
 // split-BF16 tensor-core form of the complex stage (strack_cmplx_tc.cu)
 bool cmplx_tc_supported(int W);
+int cmplx_tc_threads();  // threads per CTA of the tensor-core kernel
 int cmplx_tc_blocks_per_sm();
 cudaError_t launch_strack_cmplx_tc(const CmplxArgs& a, int nCta, cudaStream_t st);
 
