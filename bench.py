@@ -25,6 +25,7 @@ the data path); rank 0 prints the max-over-ranks time.
 """
 import argparse
 import collections
+import dataclasses
 import json
 import os
 import subprocess
@@ -381,6 +382,53 @@ def parity_other_configs(ctx):
     return out
 
 
+def throughput_other_configs(ctx, args):
+    """Throughput of the other configurations, recorded on the default bench
+    line so that the same run measures them: cfg1 (strack 1024 x 2048, W 32),
+    cfg3 (strackw 8000 x 16000 shear, search 224), cfg4 (256 heterogeneous
+    tiles + cullst) and cfg5 (serving), each with one warm-up pass and a short
+    timed run.  A failure is recorded as a string and does not stop the line."""
+    import copy
+    import torch
+    from specklesource_b200 import abi, synth
+    out = {}
+    try:
+        s1, s2 = synth.small_pair(device="cuda", na=1024, nr=2048)
+        g1 = abi.TrackParams(rStart=40, aStart=40, deltaR=16, deltaA=8, nR=124, nA=119, wR=32, wA=32, wRa=32,
+                             wAa=32)
+        ms = _time_calls(ctx, lambda: ctx.strack(g1, s1, s2), 20, 3)
+        out["cfg1"] = {"workload": "strack 1024x2048 w32 step 16x8, complex + fallback, device images",
+                       "patches_per_s": 124 * 119 / (np.median(ms) * 1e-3), "ms_per_call": float(np.median(ms))}
+        del s1, s2
+    except Exception as ex:  # recorded, not fatal
+        out["cfg1"] = f"failed: {ex}"
+    try:
+        na, nr = 8000, 16000
+        s1, s2 = synth.shear_pair(device="cuda", na=na, nr=nr, seed=3)
+        g3 = abi.TrackParams(rStart=160, aStart=160, deltaR=32, deltaA=32, nR=(nr - 320) // 32 + 1,
+                             nA=(na - 320) // 32 + 1, wR=224, wA=224, wRa=224, wAa=224, edgePadR=48, edgePadA=48,
+                             navgR=2, navgA=2)
+        ms = _time_calls(ctx, lambda: ctx.strackw(g3, s1, s2), 2, 1)
+        n3 = g3.nR * g3.nA
+        out["cfg3"] = {"workload": "strackw 8000x16000 shear, search 224, edge pad 48, step 32, navg 2",
+                       "points": n3, "points_per_s": n3 / (np.median(ms) * 1e-3), "ms_per_call": float(np.median(ms))}
+        del s1, s2
+        torch.cuda.empty_cache()
+    except Exception as ex:
+        out["cfg3"] = f"failed: {ex}"
+    for name, fn in (("cfg4", run_batched), ("cfg5", run_serving)):
+        try:
+            a2 = copy.copy(args)
+            a2.steps, a2.warmup = 1, 1
+            r = fn(a2)
+            r.pop("clocks", None)
+            out[name] = r
+            torch.cuda.empty_cache()
+        except Exception as ex:
+            out[name] = f"failed: {ex}"
+    return out
+
+
 # ---------------------------------------------------------------- main
 
 def pinned_big_endian(torch, t):
@@ -563,7 +611,7 @@ def run_batched(args):
     torch.cuda.synchronize()
     pts = sum(j.params.nR * j.params.nA for j in jobs)
     clocks = ClockSampler(0)
-    with serve.JobServer(slots=args.slots, hbm_budget=120e9) as srv:
+    with serve.JobServer(slots=args.slots, hbm_budget=120e9, max_batch=args.max_batch) as srv:
         # warm-up: the whole job set, so every slot holds its tables and buffers
         for _ in range(max(1, args.warmup)):
             [f.result() for f in [srv.submit(j) for j in jobs]]
@@ -596,6 +644,24 @@ def run_batched(args):
             if rep >= max(1, args.warmup):
                 bwalls.append(time.perf_counter() - t0)
         bwall = float(np.median(bwalls))
+        # breakdown, tracking only: the strack tiles on the server's slots
+        # against one sb_strack_batch call, and the strackw tiles on the slots
+        def _wall(fn):
+            ts = []
+            for rep in range(max(1, args.warmup) + max(1, args.steps)):
+                t0 = time.perf_counter()
+                fn()
+                if rep >= max(1, args.warmup):
+                    ts.append(time.perf_counter() - t0)
+            return float(np.median(ts))
+        st_track = [dataclasses.replace(j, cull=None, inject=None) for j in st_jobs]
+        sw_track = [dataclasses.replace(j, cull=None, inject=None) for j in sw_jobs]
+        t_st_srv = _wall(lambda: [f.result() for f in [srv.submit(j) for j in st_track]])
+        t_st_batch = _wall(lambda: bctx.strack_batch([j.params for j in st_jobs], [j.img1 for j in st_jobs],
+                                                     [j.img2 for j in st_jobs]))
+        t_sw_srv = _wall(lambda: [f.result() for f in [srv.submit(j) for j in sw_track]])
+        st_pts = sum(j.params.nR * j.params.nA for j in st_jobs)
+        sw_pts = sum(j.params.nR * j.params.nA for j in sw_jobs)
         bctx.close()
     n_w = collections.Counter(("strack w%d" % j.params.wR) if j.kind == "strack" else
                               ("strackw w%d" % j.params.wRa) for j in jobs)
@@ -604,11 +670,18 @@ def run_batched(args):
                         f"{args.slots} server slots", "patches": pts, "value": pts / wall,
             "unit": "patches/s (tracking + culling, wall clock)", "wall_s": wall,
             "jobs_per_s": len(jobs) / wall, "matched_fraction": matched / pts, "mix": dict(n_w),
-            "note": "jobs overlap across server slots (one CUDA stream each); "
+            "note": "jobs overlap across server slots (one CUDA stream each), a slot batching up to "
+                    f"{args.max_batch} queued strack jobs of one window into one call; "
                     f"median wall of {len(walls)} passes after {max(1, args.warmup)} warm-up passes",
             "batched": {"value": pts / bwall, "wall_s": bwall, "strack_tiles_in_one_call": len(st_jobs),
                         "what": "strack tiles in one sb_strack_batch call (stages once per window group), strackw "
                                 "tiles and every cull on the server's slots at the same time"},
+            "tracking_only": {
+                "strack_tiles": {"patches": st_pts, "server_s": t_st_srv, "batch_call_s": t_st_batch,
+                                 "server_patches_per_s": st_pts / t_st_srv,
+                                 "batch_patches_per_s": st_pts / t_st_batch},
+                "strackw_tiles": {"points": sw_pts, "server_s": t_sw_srv, "points_per_s": sw_pts / t_sw_srv},
+                "what": "no culling; median wall of the timed passes after the warm-up passes"},
             "clocks": clk}
 
 
@@ -854,6 +927,8 @@ def main():
                     help="transform form of the complex stage timed for the headline value; the other form is "
                          "measured beside it")
     ap.add_argument("--no-other-form", action="store_true", help="skip measuring the other transform form")
+    ap.add_argument("--no-other-configs", action="store_true",
+                    help="skip the cfg1/cfg3/cfg4/cfg5 throughput block of the default line")
     ap.add_argument("--slots", type=int, default=4, help="job-server slots for --workload cfg4/cfg5")
     ap.add_argument("--jobs", type=int, default=200, help="jobs offered in --workload cfg5")
     ap.add_argument("--max-batch", type=int, default=8,
@@ -987,6 +1062,9 @@ def main():
                 st_["accuracy"] = acc_forms[name]
             del a, b
             parity = parity_other_configs(ctx)
+    others = None
+    if rank == 0 and world == 1 and args.workload == "large" and not args.no_other_configs:
+        others = throughput_other_configs(ctx, args)
     if args.form == "split-bf16":
         # the split-BF16 kernel is bound by the tensor pipe: GEMM flops per patch
         # = 6 passes x 3 products x 2 x 128 x 128 x 128 (real block form)
@@ -1041,6 +1119,7 @@ def main():
                            "what": "one sb_strack call over the whole grid, images resident"},
             "accuracy": acc,
             "parity_other_configs": parity,
+            "other_configs": others,
             "gpu_launches": launches,
             "stages": {k: float(np.mean([s[k] for s in stages])) for k in stages[-1]},
             "form": args.form,

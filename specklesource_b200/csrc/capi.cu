@@ -819,6 +819,16 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
                "offsets");
             CK(cudaStreamSynchronize(c->stream), "sync");
             a.list = dlist2;
+        } else if (nC >= 8 * c->numSM * bpsm && img1->nr >= 8 * SB_BANDS_MAX) {
+            // strip order: the list grouped by range strips of image 1 (stable,
+            // so row-major inside a strip); the patches in flight then read a
+            // band of a few hundred columns that stays in L2 while the sweep
+            // moves down it, instead of whole image rows
+            const int stripPx = (img1->nr + SB_BANDS_MAX - 1) / SB_BANDS_MAX;
+            CK(launch_strip_key(dplan, dlist, nC, stripPx, SB_BANDS_MAX, dkey, c->stream), "strip_key");
+            CK(launch_partition(dkey, dlist, nC, SB_BANDS_MAX, dlist2, dpart, c->stream), "partition");
+            c->launches += 4;
+            a.list = dlist2;
         }
         const int nBand = bands.nb > 1 ? bands.nb : 1;
         // peak hand-off buffer: list chunks of at most kPeakChunk patches, each
@@ -1102,12 +1112,9 @@ extern "C" int sb_strack_batch(sb_context* c, int32_t nPairs, const sb_track_par
     }
     // ---- plans of every pair, offset into the atlases; complex lists per bucket
     const int n = (int)total;
-    std::vector<PointPlan> plan((size_t)n);
-    std::vector<int> pairOf((size_t)n), clist, gStart(nPairs);
+    std::vector<int> gStart(nPairs);
     std::vector<Bucket> buckets;
     {
-        std::vector<PointPlan> pl;
-        std::vector<int> cl;
         int g = 0;
         for (int q = 0; q < nPairs; ++q) {
             const int k = order[q];
@@ -1118,28 +1125,18 @@ extern "C" int sb_strack_batch(sb_context* c, int32_t nPairs, const sb_track_par
                 b.wRa = p->wRa;
                 b.pFirst = q;
                 b.g0 = g;
-                b.l0 = (int)clist.size();
                 buckets.push_back(b);
             }
-            plan_strack(p, I1[k].nr, I1[k].na, I2[k].nr, I2[k].na, pl, cl);
             gStart[k] = g;
-            for (size_t t = 0; t < pl.size(); ++t) {
-                PointPlan x = pl[t];
-                x.a1 += (int)rowOff[0][k];
-                x.a2 += (int)rowOff[1][k];
-                plan[(size_t)g + t] = x;
-                pairOf[(size_t)g + t] = k;
-            }
-            for (int v : cl) clist.push_back(g + v);
-            g += (int)pl.size();
+            g += p->nR * p->nA;
             buckets.back().pLast = q + 1;
             buckets.back().g1 = g;
-            buckets.back().l1 = (int)clist.size();
         }
     }
+    const int nBk = (int)buckets.size();
     PointPlan* dplan = (PointPlan*)sb_ctx_buf(c, "plan", sizeof(PointPlan) * n, &e);
     PointRec* drec = (PointRec*)sb_ctx_buf(c, "rec", sizeof(PointRec) * n, &e);
-    int* dclist = (int*)sb_ctx_buf(c, "clist", sizeof(int) * (clist.size() + 1), &e);
+    int* dclist = (int*)sb_ctx_buf(c, "clist", sizeof(int) * (n + 1), &e);
     int* dlist = (int*)sb_ctx_buf(c, "list", sizeof(int) * (n + 1), &e);
     int* dpairOf = (int*)sb_ctx_buf(c, "pairOf", sizeof(int) * n, &e);
     FitJob* dfit = (FitJob*)sb_ctx_buf(c, "fit", sizeof(FitJob) * (n + 1), &e);
@@ -1155,11 +1152,102 @@ extern "C" int sb_strack_batch(sb_context* c, int32_t nPairs, const sb_track_par
     if (!dplan || !drec || !dclist || !dlist || !dpairOf || !dfit || !dstats || !dR || !dA || !dC || !dZ || !dT ||
         !dkey || !dpart || !dAz)
         return sb_ctx_fail(c, SB_ERR_NOMEM, "device allocation failed");
-    CK(cudaMemcpyAsync(dplan, plan.data(), sizeof(PointPlan) * n, cudaMemcpyHostToDevice, c->stream), "plan");
-    CK(cudaMemcpyAsync(dpairOf, pairOf.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c->stream), "pairOf");
-    if (!clist.empty())
-        CK(cudaMemcpyAsync(dclist, clist.data(), sizeof(int) * clist.size(), cudaMemcpyHostToDevice, c->stream),
-           "clist");
+    // Plans: on the device for a polynomial shift (each complex candidate keyed
+    // by its bucket), on the host for an offset grid (its holes carry r2/a2
+    // over from point to point); then one ordered partition by bucket gives
+    // every bucket's complex list, in point order.  More buckets than the
+    // partition takes: every pair planned on the host.
+    const bool devBuckets = nBk <= PART_KMAX;
+    std::vector<std::vector<PointPlan>> hostPlans;  // alive until the stream has copied them
+    std::vector<std::vector<int>> hostKeys, hostPairs;
+    std::vector<int> clist;
+    for (int bi = 0; bi < nBk; ++bi) {
+        for (int q = buckets[bi].pFirst; q < buckets[bi].pLast; ++q) {
+            const int k = order[q];
+            const sb_track_params* p = &P[k];
+            const int m = p->nR * p->nA, g = gStart[k];
+            if (devBuckets && p->polyShift != 0) {
+                PlanArgs pa;
+                memset(&pa, 0, sizeof(pa));
+                pa.rStart = p->rStart; pa.aStart = p->aStart; pa.deltaR = p->deltaR; pa.deltaA = p->deltaA;
+                pa.nR = p->nR; pa.nA = p->nA;
+                pa.wR = p->wR; pa.wA = p->wA; pa.wRa = p->wRa; pa.wAa = p->wAa;
+                pa.scaleFactor = p->scaleFactor;
+                pa.noComplex = p->noComplex;
+                for (int t = 0; t < 3; ++t) {
+                    pa.rPoly[t] = p->rShiftPoly[t];
+                    pa.aPoly[t] = p->aShiftPoly[t];
+                }
+                pa.nr1 = I1[k].nr; pa.na1 = I1[k].na; pa.nr2 = I2[k].nr; pa.na2 = I2[k].na;
+                if (p->mask) {  // one buffer, reused in stream order
+                    const size_t mb = (size_t)p->mask->nr * p->mask->na;
+                    uint8_t* dm = (uint8_t*)sb_ctx_buf(c, "mask", mb, &e);
+                    if (!dm) return sb_ctx_fail(c, SB_ERR_NOMEM, "device allocation failed");
+                    CK(cudaMemcpyAsync(dm, p->mask->mask, mb, cudaMemcpyHostToDevice, c->stream), "mask");
+                    pa.mask = dm;
+                    pa.mR0 = p->mask->r0; pa.mA0 = p->mask->a0; pa.mNr = p->mask->nr; pa.mNa = p->mask->na;
+                    pa.mNrl = p->mask->nrl; pa.mNal = p->mask->nal;
+                }
+                pa.a1Off = (int)rowOff[0][k];
+                pa.a2Off = (int)rowOff[1][k];
+                pa.keyValue = bi;
+                pa.pairOf = dpairOf + g;
+                pa.pairId = k;
+                CK(launch_plan_poly(pa, dplan + g, dkey + g, c->stream), "plan_poly");
+                c->launches++;
+                continue;
+            }
+            std::vector<PointPlan> pl;
+            std::vector<int> cl;
+            plan_strack(p, I1[k].nr, I1[k].na, I2[k].nr, I2[k].na, pl, cl);
+            for (PointPlan& x : pl) {
+                x.a1 += (int)rowOff[0][k];
+                x.a2 += (int)rowOff[1][k];
+            }
+            if (devBuckets) {
+                std::vector<int> key((size_t)m, -1);
+                for (int v : cl) key[(size_t)v] = bi;
+                hostKeys.push_back(std::move(key));
+                CK(cudaMemcpyAsync(dkey + g, hostKeys.back().data(), sizeof(int) * m, cudaMemcpyHostToDevice,
+                                   c->stream),
+                   "keys");
+            } else {
+                for (int v : cl) clist.push_back(g + v);
+            }
+            hostPairs.push_back(std::vector<int>((size_t)m, k));
+            CK(cudaMemcpyAsync(dpairOf + g, hostPairs.back().data(), sizeof(int) * m, cudaMemcpyHostToDevice,
+                               c->stream),
+               "pairOf");
+            hostPlans.push_back(std::move(pl));
+            CK(cudaMemcpyAsync(dplan + g, hostPlans.back().data(), sizeof(PointPlan) * m, cudaMemcpyHostToDevice,
+                               c->stream),
+               "plan");
+        }
+        if (!devBuckets) buckets[bi].l1 = (int)clist.size();
+    }
+    if (devBuckets) {
+        CK(launch_partition(dkey, nullptr, n, nBk, dclist, dpart, c->stream), "partition");
+        c->launches += 3;
+        std::vector<int> keyOff((size_t)nBk + 1);
+        CK(cudaMemcpyAsync(keyOff.data(), dpart + partition_keyoff_at(n, nBk), sizeof(int) * (nBk + 1),
+                           cudaMemcpyDeviceToHost, c->stream),
+           "offsets");
+        CK(cudaStreamSynchronize(c->stream), "sync");
+        for (int bi = 0; bi < nBk; ++bi) {
+            buckets[bi].l0 = keyOff[(size_t)bi];
+            buckets[bi].l1 = keyOff[(size_t)bi + 1];
+        }
+    } else {
+        int l = 0;
+        for (int bi = 0; bi < nBk; ++bi) {  // l0 of each bucket: where the previous one ended
+            buckets[bi].l0 = l;
+            l = buckets[bi].l1;
+        }
+        if (!clist.empty())
+            CK(cudaMemcpyAsync(dclist, clist.data(), sizeof(int) * clist.size(), cudaMemcpyHostToDevice, c->stream),
+               "clist");
+        CK(cudaStreamSynchronize(c->stream), "sync");
+    }
     CK(cudaMemsetAsync(dstats, 0, sizeof(unsigned long long) * 8 * nPairs, c->stream), "memset");
     cudaEventRecord(c->ev[1], c->stream);
     CK(launch_rec_init(drec, n, c->stream), "rec_init");

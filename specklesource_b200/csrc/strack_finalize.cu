@@ -153,8 +153,11 @@ __global__ void plan_poly_kernel(PlanArgs a, PointPlan* plan, int* key)
         if (inb(r1a, a1a, a.wRa * s, a.wAa * s, a.nr1, a.na1) && inb(r2a, a2a, a.wRa * s, a.wAa * s, a.nr2, a.na2))
             pl.flags |= (s == 1 ? PF_SBOUND : PF_LBOUND);
     }
+    pl.a1 += a.a1Off;  // bounds are checked in the pair's own coordinates
+    pl.a2 += a.a2Off;
     plan[p] = pl;
-    key[p] = ((pl.flags & PF_CBOUND) && (pl.flags & PF_MASK) && a.noComplex == 0) ? 0 : -1;
+    key[p] = ((pl.flags & PF_CBOUND) && (pl.flags & PF_MASK) && a.noComplex == 0) ? a.keyValue : -1;
+    if (a.pairOf) a.pairOf[p] = a.pairId;
 }
 
 cudaError_t launch_plan_poly(const PlanArgs& a, PointPlan* plan, int* key, cudaStream_t st)
@@ -188,6 +191,24 @@ cudaError_t launch_band_key(const PointPlan* plan, const int* list, int n, int W
     if (nb < 1 || nb > SB_BANDS_MAX) return cudaErrorInvalidValue;
     if (n == 0) return cudaSuccess;
     band_key_kernel<<<(n + 255) / 256, 256, 0, st>>>(plan, list, n, W, rows1, rows2, nb, bandOf);
+    return cudaGetLastError();
+}
+
+__global__ void strip_key_kernel(const PointPlan* plan, const int* list, int n, int stripPx, int nStrips, int* key)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int s = plan[list[i]].r1 / stripPx;
+    s = s < 0 ? 0 : s;
+    key[i] = s < nStrips ? s : nStrips - 1;
+}
+
+cudaError_t launch_strip_key(const PointPlan* plan, const int* list, int n, int stripPx, int nStrips, int* key,
+                             cudaStream_t st)
+{
+    if (nStrips < 1 || nStrips > SB_BANDS_MAX || stripPx < 1) return cudaErrorInvalidValue;
+    if (n == 0) return cudaSuccess;
+    strip_key_kernel<<<(n + 255) / 256, 256, 0, st>>>(plan, list, n, stripPx, nStrips, key);
     return cudaGetLastError();
 }
 

@@ -14,9 +14,16 @@ struct PlanArgs {
     int nr1, na1, nr2, na2;
     const uint8_t* mask;  // device copy of the mask, or nullptr
     int mR0, mA0, mNr, mNa, mNrl, mNal;
+    // batched calls (zero otherwise): the pair's first image rows in the
+    // atlases, the key its complex candidates get, and the pair index to
+    // record per point (pairOf, when non-null)
+    int a1Off, a2Off;
+    int keyValue;
+    int* pairOf;
+    int pairId;
 };
 
-// Writes the plan of every point and key[p] = 0 for complex candidates, else -1.
+// Writes the plan of every point and key[p] = keyValue for complex candidates, else -1.
 cudaError_t launch_plan_poly(const PlanArgs& a, PointPlan* plan, int* key, cudaStream_t st);
 
 cudaError_t launch_rec_init(PointRec* rec, int n, cudaStream_t st);
@@ -26,6 +33,10 @@ cudaError_t launch_rec_init(PointRec* rec, int n, cudaStream_t st);
 constexpr int SB_BANDS_MAX = 32;
 cudaError_t launch_band_key(const PointPlan* plan, const int* list, int n, int W, int rows1, int rows2, int nb,
                             int* bandOf, cudaStream_t st);
+// Range strip of every complex-list entry (image-1 column r1 / stripPx, at
+// most nStrips - 1): the key of the strip-ordered complex list.
+cudaError_t launch_strip_key(const PointPlan* plan, const int* list, int n, int stripPx, int nStrips, int* key,
+                             cudaStream_t st);
 // key[p] = 0 for the points whose next missing try is `stage`, else -1.
 cudaError_t launch_select(const PointPlan* plan, const PointRec* rec, int n, const WalkParams& w, int stage,
                           int* key, cudaStream_t st);
