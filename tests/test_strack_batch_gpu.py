@@ -79,3 +79,26 @@ def test_batch_rejects_mixed_flags(ctx):
     cases[1][0].hanningFlag = 0
     with pytest.raises(SpeckleError, match="same for every pair"):
         ctx.strack_batch([c[0] for c in cases], [c[1] for c in cases], [c[2] for c in cases])
+
+
+def test_batch_more_buckets_than_partition_keys(ctx):
+    """35 (complex, amplitude) window buckets, above the 32 keys of one
+    ordered partition: the batch plans every pair on the host and must still
+    equal each pair's own call."""
+    cases = []
+    k = 0
+    for W in (16, 24, 32, 48, 64):
+        for WA in (16, 24, 32, 48, 64, 96, 128):
+            s1, s2 = synth.small_pair(device="cuda", na=400, nr=400, seed=200 + k)
+            p = abi.TrackParams(rStart=80, aStart=80, deltaR=24, deltaA=24, nR=11, nA=11, wR=W, wA=W, wRa=WA,
+                                wAa=WA, maxTries=1)
+            cases.append((p, s1, s2))
+            k += 1
+    single = [ctx.strack(p, a, b) for p, a, b in cases]
+    batch = ctx.strack_batch([c[0] for c in cases], [c[1] for c in cases], [c[2] for c in cases])
+    for k, (s, t) in enumerate(zip(single, batch)):
+        for key in ("offR", "offA", "corr", "azd", "type"):
+            sv = s[key].cpu().numpy() if hasattr(s[key], "cpu") else s[key]
+            tv = t[key].cpu().numpy() if hasattr(t[key], "cpu") else t[key]
+            assert np.array_equal(sv, tv, equal_nan=True), (k, key)
+        assert s["stats"] == t["stats"], k
