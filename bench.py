@@ -1012,9 +1012,9 @@ def main():
             o_ms.append(t)
             o_cm.append(st["cmplx_ms"])
         barrier()
-        om = max_over_ranks(torch, float(np.mean(o_ms)), world, "cuda")
+        om = max_over_ranks(torch, float(np.median(o_ms)), world, "cuda")
         form_stats[other] = {"ms_per_call": om, "patches_per_s": job_rate(world, N_A * N_R, om),
-                             "cmplx_ms": float(np.mean(o_cm)),
+                             "cmplx_ms": float(np.median(o_cm)), "timing": f"median of {args.steps} calls",
                              "ran": "split-bf16" if ctx.last_form() == abi.SB_FORM_SPLIT_BF16 else "fp32"}
         outputs[other] = {k: out[k].cpu().numpy() for k in ("offR", "offA", "corr", "type")}
         ctx.set_form(forms[args.form])

@@ -706,10 +706,17 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
             pa.mR0 = p->mask->r0; pa.mA0 = p->mask->a0; pa.mNr = p->mask->nr; pa.mNa = p->mask->na;
             pa.mNrl = p->mask->nrl; pa.mNal = p->mask->nal;
         }
+        // A large grid's complex list is grouped into range strips of image 1
+        // (stable, so row-major inside a strip): the patches in flight then
+        // read a band of a few hundred columns that stays in L2 while the
+        // sweep moves down it, instead of whole image rows.
+        const bool strips = n >= 16 * c->numSM && img1->nr >= 8 * SB_BANDS_MAX;
+        const int K = strips ? SB_BANDS_MAX : 1;
+        pa.stripPx = strips ? (img1->nr + SB_BANDS_MAX - 1) / SB_BANDS_MAX : 0;
         CK(launch_plan_poly(pa, dplan, dkey, c->stream), "plan_poly");
-        CK(launch_partition(dkey, nullptr, n, 1, dlist, dpart, c->stream), "partition");
+        CK(launch_partition(dkey, nullptr, n, K, dlist, dpart, c->stream), "partition");
         c->launches += 4;
-        CK(cudaMemcpyAsync(&nC, dpart + partition_keyoff_at(n, 1) + 1, sizeof(int), cudaMemcpyDeviceToHost,
+        CK(cudaMemcpyAsync(&nC, dpart + partition_keyoff_at(n, K) + K, sizeof(int), cudaMemcpyDeviceToHost,
                            c->stream),
            "count");
         CK(cudaStreamSynchronize(c->stream), "sync");
@@ -818,16 +825,6 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
                                sizeof(int) * (bands.nb + 1), cudaMemcpyDeviceToHost, c->stream),
                "offsets");
             CK(cudaStreamSynchronize(c->stream), "sync");
-            a.list = dlist2;
-        } else if (nC >= 8 * c->numSM * bpsm && img1->nr >= 8 * SB_BANDS_MAX) {
-            // strip order: the list grouped by range strips of image 1 (stable,
-            // so row-major inside a strip); the patches in flight then read a
-            // band of a few hundred columns that stays in L2 while the sweep
-            // moves down it, instead of whole image rows
-            const int stripPx = (img1->nr + SB_BANDS_MAX - 1) / SB_BANDS_MAX;
-            CK(launch_strip_key(dplan, dlist, nC, stripPx, SB_BANDS_MAX, dkey, c->stream), "strip_key");
-            CK(launch_partition(dkey, dlist, nC, SB_BANDS_MAX, dlist2, dpart, c->stream), "partition");
-            c->launches += 4;
             a.list = dlist2;
         }
         const int nBand = bands.nb > 1 ? bands.nb : 1;

@@ -156,7 +156,9 @@ __global__ void plan_poly_kernel(PlanArgs a, PointPlan* plan, int* key)
     pl.a1 += a.a1Off;  // bounds are checked in the pair's own coordinates
     pl.a2 += a.a2Off;
     plan[p] = pl;
-    key[p] = ((pl.flags & PF_CBOUND) && (pl.flags & PF_MASK) && a.noComplex == 0) ? a.keyValue : -1;
+    int kv = a.keyValue;
+    if (a.stripPx > 0) kv = min(max(r1, 0) / a.stripPx, SB_BANDS_MAX - 1);
+    key[p] = ((pl.flags & PF_CBOUND) && (pl.flags & PF_MASK) && a.noComplex == 0) ? kv : -1;
     if (a.pairOf) a.pairOf[p] = a.pairId;
 }
 
@@ -191,24 +193,6 @@ cudaError_t launch_band_key(const PointPlan* plan, const int* list, int n, int W
     if (nb < 1 || nb > SB_BANDS_MAX) return cudaErrorInvalidValue;
     if (n == 0) return cudaSuccess;
     band_key_kernel<<<(n + 255) / 256, 256, 0, st>>>(plan, list, n, W, rows1, rows2, nb, bandOf);
-    return cudaGetLastError();
-}
-
-__global__ void strip_key_kernel(const PointPlan* plan, const int* list, int n, int stripPx, int nStrips, int* key)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    int s = plan[list[i]].r1 / stripPx;
-    s = s < 0 ? 0 : s;
-    key[i] = s < nStrips ? s : nStrips - 1;
-}
-
-cudaError_t launch_strip_key(const PointPlan* plan, const int* list, int n, int stripPx, int nStrips, int* key,
-                             cudaStream_t st)
-{
-    if (nStrips < 1 || nStrips > SB_BANDS_MAX || stripPx < 1) return cudaErrorInvalidValue;
-    if (n == 0) return cudaSuccess;
-    strip_key_kernel<<<(n + 255) / 256, 256, 0, st>>>(plan, list, n, stripPx, nStrips, key);
     return cudaGetLastError();
 }
 

@@ -21,6 +21,9 @@ struct PlanArgs {
     int keyValue;
     int* pairOf;
     int pairId;
+    // > 0: complex candidates are keyed by their range strip of image 1,
+    // min(r1 / stripPx, SB_BANDS_MAX - 1), instead of keyValue
+    int stripPx;
 };
 
 // Writes the plan of every point and key[p] = keyValue for complex candidates, else -1.
@@ -33,10 +36,6 @@ cudaError_t launch_rec_init(PointRec* rec, int n, cudaStream_t st);
 constexpr int SB_BANDS_MAX = 32;
 cudaError_t launch_band_key(const PointPlan* plan, const int* list, int n, int W, int rows1, int rows2, int nb,
                             int* bandOf, cudaStream_t st);
-// Range strip of every complex-list entry (image-1 column r1 / stripPx, at
-// most nStrips - 1): the key of the strip-ordered complex list.
-cudaError_t launch_strip_key(const PointPlan* plan, const int* list, int n, int stripPx, int nStrips, int* key,
-                             cudaStream_t st);
 // key[p] = 0 for the points whose next missing try is `stage`, else -1.
 cudaError_t launch_select(const PointPlan* plan, const PointRec* rec, int n, const WalkParams& w, int stage,
                           int* key, cudaStream_t st);
