@@ -60,6 +60,7 @@ __device__ __forceinline__ int cpeak_plane(const float* mag, float pmax, unsigne
     unsigned best = 0xffffffffu;
     for (int e = tid; e < N * N / 4; e += NT) {
         const float4 v = reinterpret_cast<const float4*>(mag)[e];
+        if (fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w)) < lo) continue;  // candidates are rare
         const float vv[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
         for (int c = 0; c < 4; ++c) {

@@ -125,17 +125,33 @@ __device__ __forceinline__ void cpeak_from_planes(const float* smf, float pmax, 
     const float lo = pm * (1.0f - 1.0f / 1048576.0f);
     unsigned best = 0xffffffffu;
     constexpr int Q4 = W * W / 4;  // float4 per plane
-    for (int e = tid; e < 4 * Q4; e += NT) {
-        const int q = e / Q4, i4 = e - q * Q4;
-        const float4 v = reinterpret_cast<const float4*>(smf + poff<W>(q))[i4];
-        const float vv[4] = {v.x, v.y, v.z, v.w};
+    constexpr int U = 4;           // float4 loads in flight per thread
+    for (int e0 = tid; e0 < 4 * Q4; e0 += U * NT) {
+        float4 v[U];
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            if (vv[c] >= lo && sqrtf(vv[c]) == sm) {
-                const int idx = 4 * i4 + c;
-                const int cy = 2 * (idx / W) + (q >> 1), cx = 2 * (idx % W) + (q & 1);
-                const int y = cy < W ? cy + W : cy - W, x = cx < W ? cx + W : cx - W;
-                best = min(best, (unsigned)cpeak_rank(y, x, W));
+        for (int u = 0; u < U; ++u) {
+            const int e = e0 + u * NT;
+            const int q = e / Q4, i4 = e - q * Q4;
+            v[u] = e < 4 * Q4 ? reinterpret_cast<const float4*>(smf + poff<W>(q))[i4]
+                              : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            // candidates are rare: one test per float4 keeps the sqrtf and
+            // the rank work off the common path (the compiler predicates a
+            // plain per-value test, sqrtf included)
+            if (fmaxf(fmaxf(v[u].x, v[u].y), fmaxf(v[u].z, v[u].w)) < lo) continue;
+            const int e = e0 + u * NT;
+            const int q = e / Q4, i4 = e - q * Q4;
+            const float vv[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                if (vv[c] >= lo && sqrtf(vv[c]) == sm) {
+                    const int idx = 4 * i4 + c;
+                    const int cy = 2 * (idx / W) + (q >> 1), cx = 2 * (idx % W) + (q & 1);
+                    const int y = cy < W ? cy + W : cy - W, x = cx < W ? cx + W : cx - W;
+                    best = min(best, (unsigned)cpeak_rank(y, x, W));
+                }
             }
         }
     }

@@ -590,8 +590,9 @@ __global__ void __launch_bounds__(tcf::NT, 2) strack_cmplx_tc_kernel(CmplxArgs a
                 const float lo = pm * (1.0f - 1.0f / 1048576.0f);
                 unsigned best = 0xffffffffu;
                 const int e2 = w, m1 = k;
+                // only a thread whose own maximum reaches lo holds candidates
 #pragma unroll 1
-                for (int e1 = 0; e1 < 2; ++e1) {
+                for (int e1 = 0; e1 < (pmax >= lo ? 2 : 0); ++e1) {
                     const int q = 2 * e1 + e2;
 #pragma unroll
                     for (int c4 = 0; c4 < 8; ++c4) {
