@@ -21,6 +21,8 @@
 // W = 32), measured per window.
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "strack_device.cuh"
 #include "strack_kernels.h"
 
@@ -74,6 +76,23 @@ __device__ __forceinline__ float2 load_sample_t(const void* __restrict__ img, in
     } else {
         uint32_t w = __ldg(reinterpret_cast<const uint32_t*>(img) + k);
         if (byteOrder == SB_MSB) w = bswap16x2(w);
+        return make_float2((float)(int16_t)(w & 0xffffu), (float)(int16_t)(w >> 16));
+    }
+}
+
+// A raw sample (as load_sample_t reads it) to complex float: byte swap for
+// big-endian files, complex float32 scaled by 1000 (getPatches), int16 as is.
+template <bool F32>
+__device__ __forceinline__ float2 decode_sample(typename std::conditional<F32, uint2, uint32_t>::type w, bool msb)
+{
+    if constexpr (F32) {
+        if (msb) {
+            w.x = bswap32(w.x);
+            w.y = bswap32(w.y);
+        }
+        return make_float2(__uint_as_float(w.x) * 1000.f, __uint_as_float(w.y) * 1000.f);
+    } else {
+        if (msb) w = bswap16x2(w);
         return make_float2((float)(int16_t)(w & 0xffffu), (float)(int16_t)(w >> 16));
     }
 }
@@ -336,22 +355,50 @@ __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(Cmp
     const float thrAll = thr * W * W;
     const int jc = tid % W, i0 = (tid / W) * RPT;  // load phase: column jc, rows i0 .. i0+RPT-1
 
-    for (int it = blockIdx.x; it < a.nList; it += gridDim.x) {
-        const int p = a.list[it];
-        const PointPlan pl = a.plan[p];
+    // list entries are loaded two patches ahead and plans one patch ahead,
+    // so a patch's window loads never wait on the dependent list -> plan loads
+    const int G = gridDim.x;
+    int pNext = a.list[blockIdx.x];
+    int pAfter = (int)blockIdx.x + G < a.nList ? a.list[blockIdx.x + G] : 0;
+    PointPlan plNext = a.plan[pNext];
+    for (int it = blockIdx.x; it < a.nList; it += G) {
+        const int p = pNext;
+        const PointPlan pl = plNext;
+        if (it + G < a.nList) {
+            pNext = pAfter;
+            plNext = a.plan[pAfter];
+            if (it + 2 * G < a.nList) pAfter = a.list[it + 2 * G];
+        }
         // ---------------------------------------------------- getPatches
         // per-thread partial sums over the RPT rows in float, block totals in double
         float f[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         int nLow = 0;
+        // batches of LB rows: every load of a batch is issued before any is
+        // used (the Hanning taper and the byte order are predicates, not
+        // branches, so nothing stops the compiler from hoisting them)
+        constexpr int LB = RPT < 8 ? RPT : 8;
+        const bool msb = a.byteOrder == SB_MSB;
+        const bool han = a.hanning != nullptr;
 #pragma unroll
-        for (int r = 0; r < RPT; ++r) {
-            const int i = i0 + r;
-            float2 z1 = load_sample_t<F32>(a.img1, a.nr1, pl.a1 + i, pl.r1 + jc, a.byteOrder);
-            float2 z2 = load_sample_t<F32>(a.img2, a.nr2, pl.a2 + i, pl.r2 + jc, a.byteOrder);
-            if (a.hanning) {
-                const float h = __ldg(a.hanning + i * W + jc);
-                z2.x *= h;
-                z2.y *= h;
+        for (int r0 = 0; r0 < RPT; r0 += LB) {
+            using Raw = typename std::conditional<F32, uint2, uint32_t>::type;
+            Raw w1[LB], w2[LB];
+            float hv[LB];
+#pragma unroll
+            for (int u = 0; u < LB; ++u) {
+                const int i = i0 + r0 + u;
+                w1[u] = __ldg(reinterpret_cast<const Raw*>(a.img1) + ((size_t)(pl.a1 + i) * a.nr1 + pl.r1 + jc));
+                w2[u] = __ldg(reinterpret_cast<const Raw*>(a.img2) + ((size_t)(pl.a2 + i) * a.nr2 + pl.r2 + jc));
+                hv[u] = han ? __ldg(a.hanning + i * W + jc) : 1.f;
+            }
+#pragma unroll
+            for (int u = 0; u < LB; ++u) {
+            const int i = i0 + r0 + u;
+            float2 z1 = decode_sample<F32>(w1[u], msb);
+            float2 z2 = decode_sample<F32>(w2[u], msb);
+            if (han) {
+                z2.x *= hv[u];
+                z2.y *= hv[u];
             }
             const float pw1 = __fadd_rn(__fmul_rn(z1.x, z1.x), __fmul_rn(z1.y, z1.y));
             const float pw2 = __fadd_rn(__fmul_rn(z2.x, z2.x), __fmul_rn(z2.y, z2.y));
@@ -364,6 +411,7 @@ __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(Cmp
             f[5] += z2.y;
             X[i * RS + jc] = z1;
             Z[i * RS + jc] = z2;
+            }
         }
         double s[7] = {f[0], f[1], f[2], f[3], f[4], f[5], (double)nLow};
         block_allsum<7, NT>(s, red);

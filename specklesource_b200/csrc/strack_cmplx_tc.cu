@@ -367,9 +367,20 @@ __global__ void __launch_bounds__(tcf::NT, 2) strack_cmplx_tc_kernel(CmplxArgs a
     const float thr = F32 ? 1e-15f : 1e-9f;
     const float thrAll = thr * W * W;
 
-    for (int it = blockIdx.x; it < a.nList && !failed; it += gridDim.x) {
-        const int p = a.list[it];
-        const PointPlan pl = a.plan[p];
+    // list entries two patches ahead, plans one patch ahead (no dependent
+    // list -> plan -> window load chain at the start of a patch)
+    const int G = gridDim.x;
+    int pNext = a.list[blockIdx.x];
+    int pAfter = (int)blockIdx.x + G < a.nList ? a.list[blockIdx.x + G] : 0;
+    PointPlan plNext = a.plan[pNext];
+    for (int it = blockIdx.x; it < a.nList && !failed; it += G) {
+        const int p = pNext;
+        const PointPlan pl = plNext;
+        if (it + G < a.nList) {
+            pNext = pAfter;
+            plNext = a.plan[pAfter];
+            if (it + 2 * G < a.nList) pAfter = a.list[it + 2 * G];
+        }
         // ------------------------------------------------ getPatches: column k of window w, rows [32 h, 32 h + 32)
         // power / mean sums in float per thread, totals in double; lag-1 sums
         // along azimuth in double (mean-corrected after the reduction)
