@@ -931,8 +931,10 @@ def main():
                     help="skip the cfg1/cfg3/cfg4/cfg5 throughput block of the default line")
     ap.add_argument("--slots", type=int, default=4, help="job-server slots for --workload cfg4/cfg5")
     ap.add_argument("--jobs", type=int, default=200, help="jobs offered in --workload cfg5")
-    ap.add_argument("--max-batch", type=int, default=8,
-                    help="job server: queued strack jobs that share one sb_strack_batch call (cfg5)")
+    ap.add_argument("--max-batch", type=int, default=1,
+                    help="job server: queued strack jobs of one window that may share one sb_strack_batch call "
+                         "(cfg4/cfg5; 1: every job its own call -- batches of varying size grow the contexts' "
+                         "buffers while timed, and a buffer's reallocation waits for the whole device)")
     ap.add_argument("--batch", type=int, default=32768, help="patches per batch in --workload dftgemm")
     ap.add_argument("--workload", default="large", choices=["large", "small", "cfg1", "cfg3", "cfg3small", "cfg4", "cfg5", "cull", "dftgemm"],
                     help="small: 2400x4800 profiling case of the same generator; cfg1 / cfg3 / cull: the "

@@ -182,16 +182,38 @@ def test_same_result_alone_and_in_the_mix():
     with serve.JobServer(slots=3, hbm_budget=60e9) as srv:
         mixed = [f.result(timeout=600) for f in [srv.submit(j) for j in jobs]]
     assert len({r["slot"] for r in mixed}) > 1
-    # continuous batching: queued strack jobs share sb_strack_batch calls
-    with serve.JobServer(slots=1, hbm_budget=60e9, max_batch=4) as srv:
-        batched = [f.result(timeout=600) for f in [srv.submit(j) for j in jobs]]
-        assert max(srv.batches) > 1
-    for a, m in zip(alone, batched):
+    for a, m in zip(alone, mixed):
         for k in ("offR", "offA", "corr", "type"):
             assert np.array_equal(a["track"][k], m["track"][k], equal_nan=True), k
         for k in ("offRS", "offAS", "type"):
             assert np.array_equal(a["cull"][k], m["cull"][k], equal_nan=True), k
-    for a, m in zip(alone, mixed):
+
+
+@pytest.mark.gpu
+def test_queued_strack_jobs_share_batched_calls():
+    """Continuous batching: strack jobs of one window queued behind a busy
+    slot run together in one sb_strack_batch call, each with the result it
+    has alone (tracking and culling)."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from specklesource_b200 import build, runtime, synth
+    build.build()
+    jobs = []
+    for k, (na, nr) in enumerate([(512, 768), (640, 1024), (512, 512), (768, 768), (600, 900), (512, 1024)]):
+        s1, s2 = synth.small_pair(device="cuda", na=na, nr=nr, seed=60 + k)
+        W = 32
+        p = abi.TrackParams(rStart=W, aStart=W, deltaR=W // 2, deltaA=W // 2, nR=(nr - 2 * W) // (W // 2),
+                            nA=(na - 2 * W) // (W // 2), wR=W, wA=W, wRa=W, wAa=W)
+        jobs.append(serve.Job(kind="strack", params=p, img1=s1, img2=s2,
+                              cull=abi.CullParams(nR=p.nR, nA=p.nA, islandThresh=4), tag=k))
+    with runtime.Context(0) as ctx:
+        alone = [serve.run_job(ctx, j) for j in jobs]
+    with serve.JobServer(slots=1, hbm_budget=60e9, max_batch=4) as srv:
+        batched = [f.result(timeout=600) for f in [srv.submit(j) for j in jobs]]
+        sizes = list(srv.batches)
+    assert max(sizes) > 1 and sum(sizes) == len(jobs), sizes
+    for a, m in zip(alone, batched):
         for k in ("offR", "offA", "corr", "type"):
             assert np.array_equal(a["track"][k], m["track"][k], equal_nan=True), k
         for k in ("offRS", "offAS", "type"):
