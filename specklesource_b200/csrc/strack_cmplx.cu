@@ -80,6 +80,14 @@ __device__ __forceinline__ float2 load_sample_t(const void* __restrict__ img, in
     }
 }
 
+// Rows per batch of window loads: the largest divisor of a thread's run of
+// rows that is at most 8.
+__host__ __device__ constexpr int load_batch(int rpt)
+{
+    return rpt % 8 == 0 ? 8 : rpt % 7 == 0 ? 7 : rpt % 6 == 0 ? 6 : rpt % 5 == 0 ? 5 : rpt % 4 == 0 ? 4
+           : rpt % 3 == 0 ? 3 : rpt % 2 == 0 ? 2 : 1;
+}
+
 // A raw sample (as load_sample_t reads it) to complex float: byte swap for
 // big-endian files, complex float32 scaled by 1000 (getPatches), int16 as is.
 template <bool F32>
@@ -376,7 +384,8 @@ __global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(Cmp
         // batches of LB rows: every load of a batch is issued before any is
         // used (the Hanning taper and the byte order are predicates, not
         // branches, so nothing stops the compiler from hoisting them)
-        constexpr int LB = RPT < 8 ? RPT : 8;
+        constexpr int LB = load_batch(RPT);
+        static_assert(RPT % LB == 0, "whole batches of rows");
         const bool msb = a.byteOrder == SB_MSB;
         const bool han = a.hanning != nullptr;
 #pragma unroll
