@@ -47,6 +47,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "strack_device.cuh"
 #include "strack_kernels.h"
 
@@ -257,6 +259,23 @@ __device__ __forceinline__ float2 tc_sample(const void* __restrict__ img, int nr
     }
 }
 
+// A raw sample as tc_sample reads it, to complex float (byte swap for
+// big-endian files; complex float32 scaled by 1000, int16 as is).
+template <bool F32>
+__device__ __forceinline__ float2 tc_decode(typename std::conditional<F32, uint2, uint32_t>::type w, bool msb)
+{
+    if constexpr (F32) {
+        if (msb) {
+            w.x = bswap32(w.x);
+            w.y = bswap32(w.y);
+        }
+        return make_float2(__uint_as_float(w.x) * 1000.f, __uint_as_float(w.y) * 1000.f);
+    } else {
+        if (msb) w = bswap16x2(w);
+        return make_float2((float)(int16_t)(w & 0xffffu), (float)(int16_t)(w >> 16));
+    }
+}
+
 template <bool F32>
 __global__ void __launch_bounds__(tcf::NT, 2) strack_cmplx_tc_kernel(CmplxArgs a)
 {
@@ -387,10 +406,17 @@ __global__ void __launch_bounds__(tcf::NT, 2) strack_cmplx_tc_kernel(CmplxArgs a
         const void* img = w ? a.img2 : a.img1;
         const int nr = w ? a.nr2 : a.nr1;
         const int r0 = (w ? pl.a2 : pl.a1), c0 = (w ? pl.r2 : pl.r1) + k;
-        auto sample = [&](int i) {
-            float2 v = tc_sample<F32>(img, nr, r0 + i, c0, a.byteOrder);
-            if (w && a.hanning) {
-                const float hv = __ldg(a.hanning + i * W + k);
+        // raw loads sixteen rows at a time (the taper and the byte order are
+        // predicates), decoded where they are used
+        using Raw = typename std::conditional<F32, uint2, uint32_t>::type;
+        const Raw* base = reinterpret_cast<const Raw*>(img);
+        const bool msb = a.byteOrder == SB_MSB;
+        const bool han = w && a.hanning;
+        auto raw_at = [&](int i) { return __ldg(base + ((size_t)(r0 + i) * nr + c0)); };
+        auto han_at = [&](int i) { return han ? __ldg(a.hanning + i * W + k) : 1.f; };
+        auto decode = [&](Raw wv, float hv) {
+            float2 v = tc_decode<F32>(wv, msb);
+            if (han) {
                 v.x *= hv;
                 v.y *= hv;
             }
@@ -399,18 +425,26 @@ __global__ void __launch_bounds__(tcf::NT, 2) strack_cmplx_tc_kernel(CmplxArgs a
         float fp = 0.f, fr = 0.f, fi = 0.f;
         uint32_t low = 0;  // rows of this half whose power is below the threshold
         double lr = 0, li = 0, nr_ = 0, ni_ = 0, pr_ = 0, pi_ = 0;  // sum z[i] conj z[i-1], sum z[1..], sum z[..62]
-        float2 prev = h ? sample(31) : make_float2(0.f, 0.f);      // the pair (31, 32) belongs to half 1
+        float2 prev = make_float2(0.f, 0.f);
+        if (h) prev = decode(raw_at(31), han_at(31));  // the pair (31, 32) belongs to half 1
         const uint32_t rowOff = row_kmajor(L);
 #pragma unroll 1
-        for (int g = 0; g < 4; ++g) {  // 8 rows per chunk of the K-major F1 operand
-            float2 z[8];
+        for (int g2 = 0; g2 < 4; g2 += 2) {
+            Raw wr[16];
+            float hvv[16];
 #pragma unroll
-            for (int q = 0; q < 8; ++q) z[q] = sample(32 * h + 8 * g + q);
+            for (int q = 0; q < 16; ++q) {
+                wr[q] = raw_at(32 * h + 8 * g2 + q);
+                hvv[q] = han_at(32 * h + 8 * g2 + q);
+            }
+#pragma unroll
+        for (int gg = 0; gg < 2; ++gg) {  // 8 rows per chunk of the K-major F1 operand
+            const int g = g2 + gg;
             float re[8], im[8];
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
                 const int i = 32 * h + 8 * g + q;
-                const float2 v = z[q];
+                const float2 v = decode(wr[8 * gg + q], hvv[8 * gg + q]);
                 const float pw = __fadd_rn(__fmul_rn(v.x, v.x), __fmul_rn(v.y, v.y));
                 low |= (uint32_t)(pw < thr) << (8 * g + q);
                 fp += pw;
@@ -431,6 +465,7 @@ __global__ void __launch_bounds__(tcf::NT, 2) strack_cmplx_tc_kernel(CmplxArgs a
                 im[q] = v.y;
             }
             put_chunk(A, rowOff, L & 7, 4 * h + g, re, im);
+        }
         }
         // getPatches counts the positions where either window's power is low
         lowm[2 * L + h] = low;
