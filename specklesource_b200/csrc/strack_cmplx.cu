@@ -62,24 +62,6 @@ __device__ __forceinline__ float fmap(const float* sm, int y, int x)
     return cmap<W>(sm, cy, cx);
 }
 
-template <bool F32>
-__device__ __forceinline__ float2 load_sample_t(const void* __restrict__ img, int nr, int row, int col, int byteOrder)
-{
-    const size_t k = (size_t)row * (size_t)nr + (size_t)col;
-    if constexpr (F32) {
-        uint2 w = __ldg(reinterpret_cast<const uint2*>(img) + k);
-        if (byteOrder == SB_MSB) {
-            w.x = bswap32(w.x);
-            w.y = bswap32(w.y);
-        }
-        return make_float2(__uint_as_float(w.x) * 1000.f, __uint_as_float(w.y) * 1000.f);
-    } else {
-        uint32_t w = __ldg(reinterpret_cast<const uint32_t*>(img) + k);
-        if (byteOrder == SB_MSB) w = bswap16x2(w);
-        return make_float2((float)(int16_t)(w & 0xffffu), (float)(int16_t)(w >> 16));
-    }
-}
-
 // Rows per batch of window loads: the largest divisor of a thread's run of
 // rows that is at most 8.
 __host__ __device__ constexpr int load_batch(int rpt)
@@ -88,8 +70,9 @@ __host__ __device__ constexpr int load_batch(int rpt)
            : rpt % 3 == 0 ? 3 : rpt % 2 == 0 ? 2 : 1;
 }
 
-// A raw sample (as load_sample_t reads it) to complex float: byte swap for
-// big-endian files, complex float32 scaled by 1000 (getPatches), int16 as is.
+// A raw sample (8 bytes of complex float32 or 4 of complex int16, loaded as
+// one word) to complex float: byte swap for big-endian files, complex float32
+// scaled by 1000 (getPatches), int16 as is.
 template <bool F32>
 __device__ __forceinline__ float2 decode_sample(typename std::conditional<F32, uint2, uint32_t>::type w, bool msb)
 {
