@@ -109,14 +109,24 @@ __device__ __forceinline__ float2 sw_sample(const void* img, int nr, int na, int
 template <int W>
 struct SwCfg {
     static constexpr int N = 2 * W;
-    static constexpr int NT = W >= 96 ? 384 : 256;  // 12 warps x 80 registers beat 8 x 128 from W = 96 up
+    // 256 threads with three CTAs per SM from W = 96 to 192 (a third CTA
+    // beat 384 threads at two: 32.1 against 40.0 ms at W = 128, 76.4 against
+    // 79.2 at 192 on the 2000 x 4000 shear pair); 384 threads at two CTAs at
+    // 224 and 256 (114.3 against 116.9 ms at 224)
+    static constexpr int NT = W >= 224 ? 384 : 256;
     static constexpr int TILE = sbfft::StagedTile<N, true>::elems > sbfft::StagedTile<W, true>::elems
                                     ? sbfft::StagedTile<N, true>::elems
                                     : sbfft::StagedTile<W, true>::elems;
     static constexpr int TILEB = TILE;  // out-of-place tile of the three-step transforms
-    static constexpr size_t smem = sizeof(float2) * (TILE + TILEB + W + N + W) + sizeof(double) * (W_OSW * W_N1) +
-                                   sizeof(double) * (W_N1 * W_N1 + W_N1 * W_OSW) + sizeof(double) * (NT / 32 + 1) * 8 +
+    // oversampling kernel B (64 x 21), block X (21 x 21) and T (21 x 64), doubles
+    static constexpr int OSD = W_OSW * W_N1 + W_N1 * W_N1 + W_N1 * W_OSW;
+    // from W = 96 up they live in the (then idle) tiles, so that three CTAs fit an SM
+    static constexpr bool OS_IN_TILE = 2 * TILE >= OSD;
+    static constexpr size_t smem = sizeof(float2) * (TILE + TILEB + W + N + W) +
+                                   (OS_IN_TILE ? 0 : sizeof(double) * OSD) + sizeof(double) * (NT / 32 + 1) * 8 +
                                    sizeof(int) * (3 * (NT / 32) + 8) + 64;
+    // CTAs per SM (228 KB of shared memory, 1 KB reserved per CTA)
+    static constexpr int CTAS = W >= 96 && W <= 192 && OS_IN_TILE && 3 * (smem + 1024) <= 228 * 1024 ? 3 : 2;
     static_assert((NT / 32) * 2 * N <= W * W, "per-warp prefix slices must fit in `work`");
     // workspace (float2 units): F1, F2, work (W^2 each), I1, I2 (N^2 floats
     // each), z (N^2), row sums RS1, RS2 (N x L doubles each), meanS, sigmaS,
@@ -129,7 +139,7 @@ struct SwCfg {
 };
 
 template <int W>
-__global__ void __launch_bounds__(SwCfg<W>::NT, 2) strackw_kernel(SwArgs a)
+__global__ void __launch_bounds__(SwCfg<W>::NT, SwCfg<W>::CTAS) strackw_kernel(SwArgs a)
 {
     using C = SwCfg<W>;
     constexpr int N = C::N, NT = C::NT;
@@ -139,10 +149,11 @@ __global__ void __launch_bounds__(SwCfg<W>::NT, 2) strackw_kernel(SwArgs a)
     float2* twW = tileB + C::TILEB;
     float2* twN = twW + W;
     float2* tau = twN + N;
-    double* Bm = reinterpret_cast<double*>(tau + W);      // 64 x 21
+    double* osBase = C::OS_IN_TILE ? reinterpret_cast<double*>(tile) : reinterpret_cast<double*>(tau + W);
+    double* Bm = osBase;                                    // 64 x 21
     double* X = Bm + W_OSW * W_N1;                          // 21 x 21 block
     double* T = X + W_N1 * W_N1;                            // 21 x 64
-    double* red = T + W_N1 * W_OSW;
+    double* red = C::OS_IN_TILE ? reinterpret_cast<double*>(tau + W) : T + W_N1 * W_OSW;
     int* isc = reinterpret_cast<int*>(red + (NT / 32 + 1) * 8);
     const int tid = threadIdx.x;
 
@@ -159,7 +170,8 @@ __global__ void __launch_bounds__(SwCfg<W>::NT, 2) strackw_kernel(SwArgs a)
         sincospi(-2.0 * e / N, &s, &c);
         twN[e] = make_float2((float)c, (float)s);
     }
-    for (int e = tid; e < W_OSW * W_N1; e += NT) Bm[e] = a.B[e];
+    if constexpr (!C::OS_IN_TILE)
+        for (int e = tid; e < W_OSW * W_N1; e += NT) Bm[e] = a.B[e];
     __syncthreads();
 
     const int eR = a.eR, eA = a.eA;
@@ -479,6 +491,8 @@ __global__ void __launch_bounds__(SwCfg<W>::NT, 2) strackw_kernel(SwArgs a)
             continue;
         }
         const int iMax = best.rank / L, jMax = best.rank % L;
+        if constexpr (C::OS_IN_TILE)  // the tiles are idle until the next point's transforms
+            for (int e = tid; e < W_OSW * W_N1; e += NT) Bm[e] = __ldg(a.B + e);
         for (int e = tid; e < W_N1 * W_N1; e += NT) {
             const int bi = e / W_N1, bj = e % W_N1;
             X[e] = ncc[(size_t)(iMax - W_NFAST / 2 + bi) * L + (jMax - W_NFAST / 2 + bj)];
@@ -549,6 +563,20 @@ static cudaError_t launch_sw(const SwArgs& a, int nCta, cudaStream_t st)
     if (e != cudaSuccess) return e;
     strackw_kernel<W><<<nCta, C::NT, C::smem, st>>>(a);
     return cudaGetLastError();
+}
+
+static int sw_ctas(int W)
+{
+    switch (W) {
+    case 32: return SwCfg<32>::CTAS;
+    case 48: return SwCfg<48>::CTAS;
+    case 64: return SwCfg<64>::CTAS;
+    case 96: return SwCfg<96>::CTAS;
+    case 128: return SwCfg<128>::CTAS;
+    case 192: return SwCfg<192>::CTAS;
+    case 224: return SwCfg<224>::CTAS;
+    default: return SwCfg<256>::CTAS;
+    }
 }
 
 static bool sw_supported(int W)
@@ -751,7 +779,7 @@ extern "C" int sb_strackw(sb_context* c, const sb_track_params* p, const sb_imag
         a.stats = dst;
         const int L = 4 * eR + 1;
         a.perCta = sw_per_cta(W, L);
-        int nCta = c->numSM * 2;
+        int nCta = c->numSM * sw_ctas(W);
         if (nCta > nl) nCta = nl;
         a.scratch = (float2*)sb_ctx_buf(c, "w_scratch", sizeof(float2) * a.perCta * nCta, &e);
         if (!a.scratch) return sb_ctx_fail(c, SB_ERR_NOMEM, "strackw workspace allocation failed");
