@@ -945,7 +945,7 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
         // small windows: everything in shared memory; larger: per-CTA
         // workspace in global memory staged through shared tiles
         const bool onChip = amps_supported(Ws);
-        int nCta = c->numSM * (onChip ? amps_ctas(c, Ws) : 2);
+        int nCta = c->numSM * (onChip ? amps_ctas(c, Ws) : amp_blocks_per_sm(Ws));
         if (nCta > cnt) nCta = cnt;
         if (nCta < 1) return sb_ctx_fail(c, SB_ERR_CUDA, "amplitude kernel cannot be resident (Ws=%d)", Ws);
         if (!onChip) {
@@ -1389,7 +1389,7 @@ extern "C" int sb_strack_batch(sb_context* c, int32_t nPairs, const sb_track_par
             a.rec = brec;
             a.fit = dfit;
             const bool onChip = amps_supported(Ws);
-            int nCta = c->numSM * (onChip ? amps_ctas(c, Ws) : 2);
+            int nCta = c->numSM * (onChip ? amps_ctas(c, Ws) : amp_blocks_per_sm(Ws));
             if (nCta > cnt) nCta = cnt;
             if (nCta < 1) return sb_ctx_fail(c, SB_ERR_CUDA, "amplitude kernel cannot be resident (Ws=%d)", Ws);
             if (!onChip) {

@@ -34,10 +34,14 @@ struct AmpCfg {
                                    sizeof(int) * (3 * (NT / 32) + 8) + 64;
     // workspace: F1, F2, work (Ws^2 each), z (N^2), mag (N^2 floats)
     static constexpr size_t scratch = (size_t)3 * WS * WS + (size_t)N * N + (size_t)N * N / 2;
+    // CTAs per SM: a third at Ws = 128 (large try of window 64: 77.1 against
+    // 91.7 ms over 6,894 points of an uncorrelated 2048 x 4096 pair); at
+    // Ws = 96 it lost (85.1 against 76.5 ms)
+    static constexpr int CTAS = NT == 256 && WS == 128 && 3 * (smem + 1024) <= 228 * 1024 ? 3 : 2;
 };
 
 template <int WS, bool GAUSS>
-__global__ void __launch_bounds__(AmpCfg<WS>::NT, 2) strack_amp_kernel(AmpArgs a)
+__global__ void __launch_bounds__(AmpCfg<WS>::NT, AmpCfg<WS>::CTAS) strack_amp_kernel(AmpArgs a)
 {
     using C = AmpCfg<WS>;
     constexpr int N = C::N, NT = C::NT;
@@ -343,6 +347,20 @@ size_t amp_scratch_elems(int Ws)
 }
 
 int amp_threads(int) { return 256; }
+
+int amp_blocks_per_sm(int Ws)
+{
+    switch (Ws) {
+    case 16: return AmpCfg<16>::CTAS;
+    case 24: return AmpCfg<24>::CTAS;
+    case 32: return AmpCfg<32>::CTAS;
+    case 48: return AmpCfg<48>::CTAS;
+    case 64: return AmpCfg<64>::CTAS;
+    case 96: return AmpCfg<96>::CTAS;
+    case 128: return AmpCfg<128>::CTAS;
+    default: return 2;
+    }
+}
 
 cudaError_t launch_strack_amp(int Ws, const AmpArgs& a, int nCta, cudaStream_t st)
 {

@@ -118,6 +118,7 @@ cudaError_t launch_strack_cmplx_tc(const CmplxArgs& a, int nCta, cudaStream_t st
 
 bool amp_supported(int Ws);
 size_t amp_scratch_elems(int Ws);
+int amp_blocks_per_sm(int Ws);  // resident CTAs per SM of the staged amplitude kernel
 int amp_threads(int Ws);
 cudaError_t launch_strack_amp(int Ws, const AmpArgs& a, int nCta, cudaStream_t st);
 
