@@ -313,7 +313,7 @@ __device__ __forceinline__ void phase_correct_int(const CmplxArgs& a, const Poin
 }
 
 template <int W, int NT, bool F32, bool GAUSS>
-__global__ void __launch_bounds__(NT, (W >= 48 ? 2 : 3)) strack_cmplx_kernel(CmplxArgs a)
+__global__ void __launch_bounds__(NT, (W >= 64 ? 2 : 3)) strack_cmplx_kernel(CmplxArgs a)
 {
     using S = CmplxSmem<W, NT>;
     constexpr int RS = S::RS, IMG = S::IMG;
