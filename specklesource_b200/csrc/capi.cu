@@ -580,6 +580,7 @@ static FitArgs make_fit_args(const sb_track_params* p, FitJob* fit, int nList, i
     FitArgs f;
     f.fit = fit;
     f.nList = nList;
+    f.nListDev = nullptr;
     f.stage = stage;
     f.wR = p->wR; f.wA = p->wA; f.wRa = p->wRa; f.wAa = p->wAa;
     f.noComplex = p->noComplex;
@@ -884,30 +885,30 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
     w.maxTries = p->maxTries;
     const bool ownAz = (p->wRa == p->wR && p->wAa == p->wA);
     int* dAz = nullptr;
-    if (nC > 0) {
-        CK(cudaStreamSynchronize(c->stream), "sync");
-        float t0 = 0, t1 = 0;
-        cudaEventElapsedTime(&t0, c->sev[0], c->sev[1]);
-        cudaEventElapsedTime(&t1, c->sev[1], c->sev[2]);
-        c->stage[0] = t0;
-        c->stage[3] += t1;
-        if (tcErrFlag) {
-            int bad = 0;
-            CK(cudaMemcpy(&bad, tcErrFlag, sizeof(int), cudaMemcpyDeviceToHost), "tcErr");
-            if (bad) return sb_ctx_fail(c, SB_ERR_TIMEOUT, "split-BF16 complex stage: a tensor-core wait timed out");
-        }
-    }
+    // The tries run without host round trips: each try's list length stays on
+    // the device (kernels launched for the whole grid read it), and the
+    // stage timings and the tensor-core wait flag are read after the call.
+    int* dStageCnt = (int*)sb_ctx_buf(c, "stageCnt", sizeof(int) * 4, &e);
+    if (!dStageCnt) return sb_ctx_fail(c, SB_ERR_NOMEM, "device allocation failed");
+    CK(cudaMemsetAsync(dStageCnt, 0, sizeof(int) * 4, c->stream), "memset");
+    bool stageRan[3] = {false, false, false};
     for (int stage = 1; stage <= 2 && stage <= p->maxTries; ++stage) {
         CK(launch_select(dplan, drec, n, w, stage, dkey, c->stream), "select");
         CK(launch_partition(dkey, nullptr, n, 1, dlist, dpart, c->stream), "partition");
         c->launches += 4;
-        int cnt = 0;
-        CK(cudaMemcpyAsync(&cnt, dpart + partition_keyoff_at(n, 1) + 1, sizeof(int), cudaMemcpyDeviceToHost,
-                           c->stream),
-           "count");
-        CK(cudaStreamSynchronize(c->stream), "sync");
-        if (cnt == 0) continue;
+        const int* dCnt = dpart + partition_keyoff_at(n, 1) + 1;
+        CK(cudaMemcpyAsync(dStageCnt + stage, dCnt, sizeof(int), cudaMemcpyDeviceToDevice, c->stream), "count");
         const int Ws = WA * (stage == 1 ? 1 : LA);
+        // small windows (shared-memory kernel): launched for the whole grid,
+        // the list length read on the device; larger windows size a per-CTA
+        // workspace by the list, so their length is read back first
+        const bool onChip = amps_supported(Ws);
+        int cnt = n;
+        if (!onChip) {
+            CK(cudaMemcpyAsync(&cnt, dCnt, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "count");
+            CK(cudaStreamSynchronize(c->stream), "sync");
+            if (cnt == 0) continue;
+        }
         const bool needFill = !ownAz && !(p->noComplex && stage == 1);
         if (needFill) {
             dAz = (int*)sb_ctx_buf(c, "azEff", sizeof(int) * n, &e);
@@ -924,7 +925,8 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
         a.byteOrder = img1->byteOrder;
         a.plan = dplan;
         a.list = dlist;
-        a.nList = cnt;
+        a.nList = cnt;  // the length, or its upper bound (the grid) when read on the device
+        a.nListDev = onChip ? dCnt : nullptr;
         a.stage = stage;
         a.s = stage == 1 ? 1 : LA;
         a.wR = p->wR; a.wA = p->wA; a.wRa = p->wRa; a.wAa = p->wAa;
@@ -944,7 +946,6 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
         a.fit = dfit;
         // small windows: everything in shared memory; larger: per-CTA
         // workspace in global memory staged through shared tiles
-        const bool onChip = amps_supported(Ws);
         int nCta = c->numSM * (onChip ? amps_ctas(c, Ws) : amp_blocks_per_sm(Ws));
         if (nCta > cnt) nCta = cnt;
         if (nCta < 1) return sb_ctx_fail(c, SB_ERR_CUDA, "amplitude kernel cannot be resident (Ws=%d)", Ws);
@@ -962,17 +963,11 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
         c->launches++;
         cudaEventRecord(c->sev[3 + 2 * stage], c->stream);
         FitArgs f = make_fit_args(p, dfit, cnt, stage, drec);
+        f.nListDev = onChip ? dCnt : nullptr;
         CK(launch_strack_fit(f, c->stream), "strack_fit");
         c->launches++;
-        CK(cudaStreamSynchronize(c->stream), "sync");
-        float t0 = 0, t1 = 0;
-        cudaEventElapsedTime(&t0, c->sev[2 + 2 * stage], c->sev[3 + 2 * stage]);
-        c->stage[stage] = t0;
-        c->stage[5 + stage] = (float)cnt;
         cudaEventRecord(c->sev[8 + stage], c->stream);
-        cudaEventSynchronize(c->sev[8 + stage]);
-        cudaEventElapsedTime(&t1, c->sev[3 + 2 * stage], c->sev[8 + stage]);
-        c->stage[3] += t1;
+        stageRan[stage] = true;
     }
     CK(launch_finalize(dplan, drec, n, w, p->scaleFactor, dR, dA, dC, dZ, dT, dstats, c->stream), "finalize");
     c->launches++;
@@ -986,8 +981,28 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
     if ((rc = out_copy(c, out->type, dT, n, out->onDevice)) != SB_OK) return rc;
     unsigned long long st[8];
     CK(cudaMemcpyAsync(st, dstats, sizeof(st), cudaMemcpyDeviceToHost, c->stream), "stats");
+    int stageCnt[4] = {0, 0, 0, 0}, tcBad = 0;
+    CK(cudaMemcpyAsync(stageCnt, dStageCnt, sizeof(stageCnt), cudaMemcpyDeviceToHost, c->stream), "counts");
+    if (tcErrFlag) CK(cudaMemcpyAsync(&tcBad, tcErrFlag, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "tcErr");
     cudaEventRecord(c->ev[3], c->stream);
     CK(cudaStreamSynchronize(c->stream), "strack");
+    if (tcBad) return sb_ctx_fail(c, SB_ERR_TIMEOUT, "split-BF16 complex stage: a tensor-core wait timed out");
+    if (nC > 0) {
+        float t0 = 0, t1 = 0;
+        cudaEventElapsedTime(&t0, c->sev[0], c->sev[1]);
+        cudaEventElapsedTime(&t1, c->sev[1], c->sev[2]);
+        c->stage[0] = t0;
+        c->stage[3] += t1;
+    }
+    for (int stage = 1; stage <= 2; ++stage) {
+        if (!stageRan[stage]) continue;
+        float t0 = 0, t1 = 0;
+        cudaEventElapsedTime(&t0, c->sev[2 + 2 * stage], c->sev[3 + 2 * stage]);
+        cudaEventElapsedTime(&t1, c->sev[3 + 2 * stage], c->sev[8 + stage]);
+        c->stage[stage] = t0;
+        c->stage[3] += t1;
+        c->stage[5 + stage] = (float)stageCnt[stage];
+    }
     out->nComplex = (int64_t)st[0];
     out->nAmp = (int64_t)st[1];
     out->nAmpL = (int64_t)st[2];
@@ -1015,6 +1030,24 @@ extern "C" int sb_strack(sb_context* c, const sb_track_params* p, const sb_image
 // is that of sb_strack, so each pair's grids equal its own sb_strack result.
 
 namespace {
+// Events owned for the duration of one batched call.
+struct BatchEvents {
+    std::vector<cudaEvent_t> ev;
+    bool good = true;
+    explicit BatchEvents(int n) : ev((size_t)n, nullptr)
+    {
+        for (auto& e : ev)
+            if (cudaEventCreate(&e) != cudaSuccess) good = false;
+    }
+    ~BatchEvents()
+    {
+        for (auto e : ev)
+            if (e) cudaEventDestroy(e);
+    }
+    bool ok() const { return good; }
+    cudaEvent_t operator[](int i) const { return ev[(size_t)i]; }
+};
+
 struct Bucket {
     int wR, wRa;
     int pFirst, pLast;           // range in the bucket order of the pairs
@@ -1251,12 +1284,20 @@ extern "C" int sb_strack_batch(sb_context* c, int32_t nPairs, const sb_track_par
     c->launches++;
 
     const int form = c->form;
+    // per-bucket complex-stage events and try counts, read after the call
+    BatchEvents bev(2 * nBk);
+    if (!bev.ok()) return sb_ctx_fail(c, SB_ERR_CUDA, "event creation failed");
+    std::vector<char> cmplxRan((size_t)nBk, 0);
+    int* dStageCnt = (int*)sb_ctx_buf(c, "stageCnt", sizeof(int) * 3 * nBk, &e);
+    if (!dStageCnt) return sb_ctx_fail(c, SB_ERR_NOMEM, "device allocation failed");
+    CK(cudaMemsetAsync(dStageCnt, 0, sizeof(int) * 3 * nBk, c->stream), "memset");
     int* dTcErr = (int*)sb_ctx_buf(c, "tcErr", sizeof(int), &e);
     if (!dTcErr) return sb_ctx_fail(c, SB_ERR_NOMEM, "device allocation failed");
     CK(cudaMemsetAsync(dTcErr, 0, sizeof(int), c->stream), "memset");
     c->lastForm = SB_FORM_FP32;
     constexpr int kPeakChunk = 1 << 19;
-    for (const Bucket& b : buckets) {
+    for (int bi = 0; bi < nBk; ++bi) {
+        const Bucket& b = buckets[bi];
         const sb_track_params* p = &P[order[b.pFirst]];  // windows and flags of the bucket
         const int W = p->wR, WA = p->wRa;
         const int nB = b.g1 - b.g0, nC = b.l1 - b.l0;
@@ -1298,7 +1339,7 @@ extern "C" int sb_strack_batch(sb_context* c, int32_t nPairs, const sb_track_par
                 dpeak = (PeakJob*)sb_ctx_buf(c, "peakjob", pc * sizeof(PeakJob), &e);
                 if (!dpeak) return sb_ctx_fail(c, SB_ERR_NOMEM, "device allocation failed");
             }
-            cudaEventRecord(c->sev[0], c->stream);
+            cudaEventRecord(bev[2 * bi], c->stream);
             for (int off = 0; off < nC; off += kPeakChunk) {
                 const int cnt = nC - off < kPeakChunk ? nC - off : kPeakChunk;
                 CmplxArgs ak = a;
@@ -1328,11 +1369,8 @@ extern "C" int sb_strack_batch(sb_context* c, int32_t nPairs, const sb_track_par
             FitArgs f = make_fit_args(p, dfit, nC, 0, drec);
             CK(launch_strack_fit(f, c->stream), "strack_fit");
             c->launches++;
-            cudaEventRecord(c->sev[1], c->stream);
-            CK(cudaEventSynchronize(c->sev[1]), "sync");
-            float t0 = 0;
-            cudaEventElapsedTime(&t0, c->sev[0], c->sev[1]);
-            c->stage[0] += t0;
+            cudaEventRecord(bev[2 * bi + 1], c->stream);
+            cmplxRan[bi] = 1;
             c->stage[5] += (float)nC;
         }
         // ---- amplitude tries over the bucket's points
@@ -1347,13 +1385,19 @@ extern "C" int sb_strack_batch(sb_context* c, int32_t nPairs, const sb_track_par
             CK(launch_select(bplan, brec, nB, w, stage, dkey, c->stream), "select");
             CK(launch_partition(dkey, nullptr, nB, 1, dlist, dpart, c->stream), "partition");
             c->launches += 4;
-            int cnt = 0;
-            CK(cudaMemcpyAsync(&cnt, dpart + partition_keyoff_at(nB, 1) + 1, sizeof(int), cudaMemcpyDeviceToHost,
-                               c->stream),
+            // the try's list length stays on the device (no host round trip)
+            const int* dCnt = dpart + partition_keyoff_at(nB, 1) + 1;
+            CK(cudaMemcpyAsync(dStageCnt + 3 * bi + stage, dCnt, sizeof(int), cudaMemcpyDeviceToDevice, c->stream),
                "count");
-            CK(cudaStreamSynchronize(c->stream), "sync");
-            if (cnt == 0) continue;
             const int Ws = WA * (stage == 1 ? 1 : LA);
+            // as in sb_strack: the length is read back only for the staged kernel
+            const bool onChip = amps_supported(Ws);
+            int cnt = nB;  // upper bound
+            if (!onChip) {
+                CK(cudaMemcpyAsync(&cnt, dCnt, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "count");
+                CK(cudaStreamSynchronize(c->stream), "sync");
+                if (cnt == 0) continue;
+            }
             const bool needFill = !ownAz && !(p->noComplex && stage == 1);
             if (needFill) {  // azShift carries over within a pair, from 0 at its first point
                 for (int q = b.pFirst; q < b.pLast; ++q) {
@@ -1373,6 +1417,7 @@ extern "C" int sb_strack_batch(sb_context* c, int32_t nPairs, const sb_track_par
             a.plan = bplan;
             a.list = dlist;
             a.nList = cnt;
+            a.nListDev = onChip ? dCnt : nullptr;
             a.stage = stage;
             a.s = stage == 1 ? 1 : LA;
             a.wR = p->wR; a.wA = p->wA; a.wRa = p->wRa; a.wAa = p->wAa;
@@ -1388,7 +1433,6 @@ extern "C" int sb_strack_batch(sb_context* c, int32_t nPairs, const sb_track_par
             a.gauss = p->gaussFlag ? 1 : 0;
             a.rec = brec;
             a.fit = dfit;
-            const bool onChip = amps_supported(Ws);
             int nCta = c->numSM * (onChip ? amps_ctas(c, Ws) : amp_blocks_per_sm(Ws));
             if (nCta > cnt) nCta = cnt;
             if (nCta < 1) return sb_ctx_fail(c, SB_ERR_CUDA, "amplitude kernel cannot be resident (Ws=%d)", Ws);
@@ -1404,9 +1448,9 @@ extern "C" int sb_strack_batch(sb_context* c, int32_t nPairs, const sb_track_par
                 CK(launch_strack_amp(Ws, a, nCta, c->stream), "strack_amp");
             c->launches++;
             FitArgs f = make_fit_args(p, dfit, cnt, stage, brec);
+            f.nListDev = onChip ? dCnt : nullptr;
             CK(launch_strack_fit(f, c->stream), "strack_fit");
             c->launches++;
-            c->stage[5 + stage] += (float)cnt;
         }
         CK(launch_finalize(bplan, brec, nB, w, p->scaleFactor, dR + b.g0, dA + b.g0, dC + b.g0, dZ + b.g0, dT + b.g0,
                            dstats, c->stream, dpairOf + b.g0),
@@ -1429,8 +1473,20 @@ extern "C" int sb_strack_batch(sb_context* c, int32_t nPairs, const sb_track_par
        "stats");
     int tcBad = 0;
     CK(cudaMemcpyAsync(&tcBad, dTcErr, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "tcErr");
+    std::vector<int> stageCnt((size_t)3 * nBk);
+    CK(cudaMemcpyAsync(stageCnt.data(), dStageCnt, sizeof(int) * 3 * nBk, cudaMemcpyDeviceToHost, c->stream),
+       "counts");
     cudaEventRecord(c->ev[3], c->stream);
     CK(cudaStreamSynchronize(c->stream), "strack_batch");
+    for (int bi = 0; bi < nBk; ++bi) {
+        if (cmplxRan[bi]) {
+            float t0 = 0;
+            cudaEventElapsedTime(&t0, bev[2 * bi], bev[2 * bi + 1]);
+            c->stage[0] += t0;
+        }
+        c->stage[6] += (float)stageCnt[(size_t)3 * bi + 1];
+        c->stage[7] += (float)stageCnt[(size_t)3 * bi + 2];
+    }
     if (tcBad) return sb_ctx_fail(c, SB_ERR_TIMEOUT, "split-BF16 complex stage: a tensor-core wait timed out");
     for (int k = 0; k < nPairs; ++k) {
         const unsigned long long* s = &st[(size_t)8 * k];

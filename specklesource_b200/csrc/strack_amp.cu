@@ -77,7 +77,8 @@ __global__ void __launch_bounds__(AmpCfg<WS>::NT, AmpCfg<WS>::CTAS) strack_amp_k
     const float scale = (float)(1. / ((size_t)WS * WS * WS * WS * OS * OS * OS));
     const int st = a.stage;
 
-    for (int it = blockIdx.x; it < a.nList; it += gridDim.x) {
+    const int nList = a.nListDev ? min(a.nList, *a.nListDev) : a.nList;
+    for (int it = blockIdx.x; it < nList; it += gridDim.x) {
         const int p = a.list[it];
         const PointPlan pl = a.plan[p];
         // window corners (computeAmpImageLocations, speckleTrack.c:147-156):

@@ -105,7 +105,8 @@ __global__ void __launch_bounds__(128) strack_fit_kernel(FitArgs a)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int job = t >> 1, f = t & 1;
-    const bool live = job < a.nList;
+    const int nList = a.nListDev ? min(a.nList, *a.nListDev) : a.nList;
+    const bool live = job < nList;
     int gate = 0;
     double s = 0.0;
     if (live) {

@@ -8,7 +8,8 @@ namespace sbk {
 
 struct FitArgs {
     const FitJob* fit;
-    int nList;
+    int nList;            // number of fit jobs, or its upper bound when nListDev is set
+    const int* nListDev;  // non-null: the number of jobs, read on the device
     int stage;  // 0 complex, 1 small amplitude, 2 large amplitude
     int wR, wA, wRa, wAa;
     int noComplex;

@@ -80,7 +80,8 @@ struct AmpArgs {
     int sampleType, byteOrder;
     const PointPlan* plan;
     const int* list;
-    int nList;
+    int nList;              // list length, or its upper bound when nListDev is set
+    const int* nListDev;    // non-null: the list length, read on the device
     int stage;   // 1 small, 2 large
     int s;       // window scale
     int wR, wA, wRa, wAa;

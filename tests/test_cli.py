@@ -90,7 +90,7 @@ def test_strack_cli_matches_library(tools, tmp_path, pair):
     assert r.returncode == 0, r.stderr
     out = files.read_track_outputs(str(tmp_path / "out"), kv["nR"], kv["nA"])
     p = abi.TrackParams(rStart=40, aStart=40, deltaR=16, deltaA=8, nR=27, nA=25, wR=32, wA=32, wRa=32, wAa=32)
-    with runtime.Context(0) as ctx:
+    with runtime.Context(0, tuning=False) as ctx:  # the tools run the default launch shapes
         g = ctx.strack(p, a, b)
     for k, q in (("dr", "offR"), ("da", "offA"), ("cc", "corr"), ("azd", "azd"), ("mt", "type")):
         assert np.array_equal(out[k], g[q]), k
@@ -121,7 +121,7 @@ def test_strack_cli_flags_reach_the_library(tools, tmp_path, pair):
     cases = [(["-gauss"], dict(gaussFlag=1)),
              (["-noComplex", "-singleAmp"], dict(noComplex=1, maxTries=1)),
              (["-noHanning", "-checkAzFocus"], dict(hanningFlag=0, checkAzFocus=1))]
-    with runtime.Context(0) as ctx:
+    with runtime.Context(0, tuning=False) as ctx:  # the tools run the default launch shapes
         for flags, kw in cases:
             r = _run(tools["strack"], flags + ["track.par"], tmp_path)
             assert r.returncode == 0, r.stderr
@@ -143,7 +143,7 @@ def test_strackw_and_cullst_cli(tools, tmp_path, pair):
     out = files.read_track_outputs(str(tmp_path / "out"), 18, 7, azd=False)
     p = abi.TrackParams(rStart=48, aStart=48, deltaR=24, deltaA=24, nR=18, nA=7, wR=32, wA=32, wRa=64, wAa=64,
                         edgePadR=8, edgePadA=8, navgR=2, navgA=2)
-    with runtime.Context(0) as ctx:
+    with runtime.Context(0, tuning=False) as ctx:  # the tools run the default launch shapes
         g = ctx.strackw(p, a, b)
         assert np.array_equal(out["dr"], g["offR"]) and np.array_equal(out["mt"], g["type"])
         # cullst on a synthetic offsets grid written in the reference's format
@@ -187,7 +187,7 @@ def test_strack_cli_interferogram(tools, tmp_path):
     full[100:] = np.array([1, 1], ">i2")
     p = abi.TrackParams(rStart=40, aStart=40, deltaR=16, deltaA=16, nR=27, nA=12, wR=32, wA=32, wRa=32, wAa=32,
                         intf=dict(data=full, nrl=4, nal=2))
-    with runtime.Context(0) as ctx:
+    with runtime.Context(0, tuning=False) as ctx:  # the tools run the default launch shapes
         g = ctx.strack(p, a, b)
     for k, q in (("dr", "offR"), ("da", "offA"), ("mt", "type")):
         assert np.array_equal(out[k], g[q]), k
