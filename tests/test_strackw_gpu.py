@@ -50,7 +50,8 @@ def _check(ctx, p, a, b):
 
 
 @pytest.mark.parametrize("W,pad,navg,n,step", [(64, 8, 1, (16, 24), 28), (64, 8, 2, (16, 24), 28),
-                                                (128, 16, 2, (14, 18), 28), (96, 12, 2, (14, 20), 30)])
+                                                (128, 16, 2, (14, 18), 28), (96, 12, 2, (14, 20), 30),
+                                                (192, 32, 2, (5, 7), 48)])
 def test_strackw_matches_oracle(ctx, shear, W, pad, navg, n, step):
     a, b = shear
     _check(ctx, _p(W, pad, navg, n=n, step=step), a, b)
