@@ -741,10 +741,15 @@ def run_serving(args):
         clk = clocks.stop()
         peak = srv.peak_bytes
     pts = sum(j.params.nR * j.params.nA for j, _ in jobs)
+    slowest = [{"side": side, "mode": "amplitude" if j.params.noComplex else "complex", "W": j.params.wR,
+                "points": j.params.nR * j.params.nA, "wait_ms": 1e3 * (r["start"] - r["arrival"]),
+                "service_ms": 1e3 * (r["end"] - r["start"])}
+               for (j, side), r in sorted(zip(jobs, res), key=lambda t: -(t[1]["end"] - t[1]["arrival"]))[:3]]
     return {"workload": f"cfg5 serving: {n_jobs} Poisson(40/s) track+cull jobs, 1024-8192 px, amplitude or "
                         f"complex, W 32-64, {args.slots} slots, 120 GB budget", "jobs": n_jobs,
             "value": n_jobs / wall, "unit": "jobs/s", "patches_per_s": pts / wall,
-            "latency_ms": serve.latency_stats(res), "offered_jobs_per_s": 40.0, "wall_s": wall,
+            "latency_ms": serve.latency_stats(res), "slowest_jobs": slowest, "offered_jobs_per_s": 40.0,
+            "wall_s": wall,
             "peak_admitted_gb": peak / 1e9, "max_batch": args.max_batch,
             "batched_job_fraction": float(np.mean([r.get("batch", 1) > 1 for r in res])), "clocks": clk}
 

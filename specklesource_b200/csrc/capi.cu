@@ -56,10 +56,12 @@ void* sb_ctx_buf(sb_context* c, const char* name, size_t bytes, cudaError_t* err
 {
     DevBuf& b = c->bufs[name];
     if (b.bytes < bytes) {
-        if (b.ptr) cudaFree(b.ptr);
+        // stream-ordered: growing a buffer does not wait for the whole device
+        // (cudaFree would), so contexts serving other jobs keep running
+        if (b.ptr) cudaFreeAsync(b.ptr, c->stream);
         b.ptr = nullptr;
         b.bytes = 0;
-        cudaError_t e = cudaMalloc(&b.ptr, bytes > 0 ? bytes : 16);
+        cudaError_t e = cudaMallocAsync(&b.ptr, bytes > 0 ? bytes : 16, c->stream);
         if (e != cudaSuccess) {
             *err = e;
             return nullptr;
@@ -117,7 +119,8 @@ extern "C" void sb_context_destroy(sb_context* c)
     cudaStreamSynchronize(c->stream);
     cudaStreamSynchronize(c->copyStream);
     for (auto& kv : c->bufs)
-        if (kv.second.ptr) cudaFree(kv.second.ptr);
+        if (kv.second.ptr) cudaFreeAsync(kv.second.ptr, c->stream);
+    cudaStreamSynchronize(c->stream);
     for (auto& kv : c->tables)
         if (kv.second) cudaFree(kv.second);
     for (int k = 0; k < 4; ++k) cudaEventDestroy(c->ev[k]);
@@ -152,8 +155,10 @@ extern "C" int sb_context_release(sb_context* c)
     cudaStreamSynchronize(c->stream);
     cudaStreamSynchronize(c->copyStream);
     for (auto& kv : c->bufs)
-        if (kv.second.ptr) cudaFree(kv.second.ptr);
+        if (kv.second.ptr) cudaFreeAsync(kv.second.ptr, c->stream);
     c->bufs.clear();
+    e = cudaStreamSynchronize(c->stream);  // the pool returns the memory at this synchronisation
+    if (e != cudaSuccess) return sb_ctx_cuda(c, e, "release");
     return SB_OK;
 }
 
@@ -523,9 +528,6 @@ static int upload_banded(sb_context* c, const sb_image* im[2], const void* dptr[
     size_t nb = hostBytes / ((size_t)16 << 20);
     b->nb = nb < 1 ? 1 : (nb > (size_t)SB_MAX_BANDS ? SB_MAX_BANDS : (int)nb);
     cudaError_t e;
-    // the copy stream must not overtake work still reading these buffers
-    cudaEventRecord(c->chunkEv[0], c->stream);
-    cudaStreamWaitEvent(c->copyStream, c->chunkEv[0], 0);
     char* dst[2] = {nullptr, nullptr};
     for (int i = 0; i < 2; ++i) {
         if (im[i]->onDevice) {
@@ -540,6 +542,10 @@ static int upload_banded(sb_context* c, const sb_image* im[2], const void* dptr[
         dptr[i] = dst[i];
         b->rows[i] = (im[i]->na + b->nb - 1) / b->nb;
     }
+    // the copy stream waits for the main stream: the buffers' (stream-ordered)
+    // allocation and any work still reading them come first
+    cudaEventRecord(c->chunkEv[0], c->stream);
+    cudaStreamWaitEvent(c->copyStream, c->chunkEv[0], 0);
     for (int k = 0; k < b->nb; ++k) {
         for (int i = 0; i < 2; ++i) {
             if (!dst[i]) continue;

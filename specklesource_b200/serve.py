@@ -311,7 +311,13 @@ def run_batch(ctx, jobs):
 
 
 def latency_stats(results):
-    """p50/p99 of arrival-to-completion latency (ms) over result dicts."""
+    """p50/p99 of arrival-to-completion latency (ms) over result dicts, split
+    into the queue wait (arrival to start) and the service time (start to
+    end) of the same jobs."""
     lat = np.array([1e3 * (r["end"] - r["arrival"]) for r in results])
+    wait = np.array([1e3 * (r["start"] - r["arrival"]) for r in results])
+    svc = lat - wait
     return {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
-            "max": float(lat.max()), "mean": float(lat.mean())}
+            "max": float(lat.max()), "mean": float(lat.mean()),
+            "wait_p50": float(np.percentile(wait, 50)), "wait_p99": float(np.percentile(wait, 99)),
+            "service_p50": float(np.percentile(svc, 50)), "service_p99": float(np.percentile(svc, 99))}

@@ -149,9 +149,10 @@ def test_queued_strack_jobs_share_a_batched_call():
 
 
 def test_latency_stats():
-    rs = [{"arrival": 0.0, "end": 0.001 * k} for k in range(1, 101)]
+    rs = [{"arrival": 0.0, "start": 0.0005 * k, "end": 0.001 * k} for k in range(1, 101)]
     st = serve.latency_stats(rs)
     assert abs(st["p50"] - 50.5) < 1e-6 and st["max"] == 100.0
+    assert abs(st["wait_p50"] - 25.25) < 1e-6 and abs(st["service_p50"] - 25.25) < 1e-6
 
 
 @pytest.mark.gpu
