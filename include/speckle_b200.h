@@ -113,7 +113,7 @@ int sb_last_form(const sb_context *ctx);
  * the resident maximum (0: that maximum).  Kernels and windows:
  *   SB_TUNE_COMPLEX     FP32 complex stage, window 16, 24, 32, 48 or 64
  *   SB_TUNE_COMPLEX_TC  split-BF16 complex stage, window 64 (threads 0)
- *   SB_TUNE_AMPLITUDE   shared-memory amplitude try, window 16, 24, 32 or 48
+ *   SB_TUNE_AMPLITUDE   shared-memory amplitude try, window 16, 24, 32, 48 or 64
  *                       (threads 0)
  * Results do not depend on ctasPerSm; a different thread count changes the
  * order of the float partial sums of the patch powers (not the transforms).

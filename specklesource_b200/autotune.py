@@ -10,7 +10,8 @@ CUDA-event timing, median of `reps` calls after a warm-up call):
     counts x every resident CTA count per SM (amplitude tries off);
   * split-BF16 complex stage, window 64: 1 or 2 CTAs per SM;
   * shared-memory amplitude try, windows 16, 24, 32, 48: every resident CTA
-    count per SM (-noComplex, one try).
+    count per SM (-noComplex, one try; window 64 fits one CTA per SM, so
+    there is nothing to choose).
 
 and writes the fastest shape per bucket, with every candidate's time, to a
 JSON table.  runtime.Context applies the table of the device it runs on

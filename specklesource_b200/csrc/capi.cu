@@ -213,7 +213,7 @@ extern "C" int sb_set_tuning(sb_context* c, int kernel, int window, int threads,
     }
     if (kernel == SB_TUNE_AMPLITUDE) {
         if (wi < 0 || !amps_supported(window) || threads != 0)
-            return sb_ctx_fail(c, SB_ERR_UNSUPPORTED, "shared-memory amplitude try: windows 16-48, default threads");
+            return sb_ctx_fail(c, SB_ERR_UNSUPPORTED, "shared-memory amplitude try: windows 16-64, default threads");
         const int mx = amps_blocks_per_sm(window);
         if (ctasPerSm > mx) return sb_ctx_fail(c, SB_ERR_ARG, "at most %d CTAs per SM", mx);
         c->tuneAmpsCtas[wi] = ctasPerSm;

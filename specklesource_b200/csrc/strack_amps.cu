@@ -1,4 +1,4 @@
-// strack_amps.cu -- amplitude tries of strack for small windows (Ws <= 48),
+// strack_amps.cu -- amplitude tries of strack for small windows (Ws <= 64),
 // one CTA per grid point with every array resident in shared memory.
 //
 // Same computation as strack_amp.cu (ampMatch / ampTrackFast,
@@ -17,7 +17,11 @@
 // the 2Ws x (2Ws+1) pair plane, ~65 KB: three CTAs per SM.  At Ws = 48 the
 // layout needs 139 KB, one CTA per SM: 192 threads with up to 255 registers
 // each (no spills) do the try 2.3x faster than the staged kernel that larger
-// windows use (strack_amp.cu); 384 threads spilled.
+// windows use (strack_amp.cu); 384 threads spilled.  At Ws = 64 the buffers
+// alone take 226.5 KB, so the lean layout keeps the twiddle, parity and
+// oversampling tables in global memory (read through L1), puts the
+// oversampling scratch in the spectrum buffer (idle by then) and sizes the
+// block reductions for four values: 232,224 bytes, one CTA per SM.
 #include <cuda_runtime.h>
 
 #include "strack_device.cuh"
@@ -32,8 +36,12 @@ struct AmpsSmem {
     static constexpr int S = WS * RS;       // one Ws buffer, float2
     static constexpr int ZS = N * (N + 1);  // pair plane, float2
     static constexpr int OSD = OSW * NFAST / 2 + 16;
-    static constexpr size_t bytes = sizeof(float2) * (3 * S + ZS + 2 * WS + N + OSD + NFAST * NFAST + NFAST * OSW) +
-                                    sizeof(float) * NFAST * NFAST + sizeof(double) * (NT / 32 + 1) * 8 + 64;
+    static constexpr size_t full = sizeof(float2) * (3 * S + ZS + 2 * WS + N + OSD + NFAST * NFAST + NFAST * OSW) +
+                                   sizeof(float) * NFAST * NFAST + sizeof(double) * (NT / 32 + 1) * 8 + 64;
+    static constexpr bool LEAN = full > 227 * 1024;
+    // lean: block_allsum of at most four values needs (warps + 1) x 4 doubles
+    static constexpr size_t bytes = LEAN ? sizeof(float2) * (3 * S + ZS) + sizeof(double) * (NT / 32 + 1) * 4 : full;
+    static_assert(bytes <= 227 * 1024, "one CTA's dynamic shared memory");
 };
 
 // Exact findCPeak over an N x N plane of |c|^2 stored at fftshifted positions
@@ -84,7 +92,7 @@ __device__ __forceinline__ int cpeak_plane(const float* mag, float pmax, unsigne
 }
 
 template <int WS, int NT, bool GAUSS>
-__global__ void __launch_bounds__(NT, (WS == 32 ? 3 : (WS == 48 ? 1 : 2))) strack_amps_kernel(AmpArgs a)
+__global__ void __launch_bounds__(NT, (WS == 32 ? 3 : (WS >= 48 ? 1 : 2))) strack_amps_kernel(AmpArgs a)
 {
     using M = AmpsSmem<WS, NT>;
     constexpr int N = M::N, RS = M::RS, S = M::S, ZR = N + 1;
@@ -95,25 +103,46 @@ __global__ void __launch_bounds__(NT, (WS == 32 ? 3 : (WS == 48 ? 1 : 2))) strac
     float2* R0 = F + S;
     float2* X = R0 + S;
     float2* z = X + S;
-    float2* twWs = z + M::ZS;
-    float2* tau = twWs + WS;
-    float2* twN = tau + WS;
-    float2* osD2 = twN + N;  // 16-byte aligned: every region before it has an even float2 count
-    float2* Yb = osD2 + M::OSD;
-    float2* T = Yb + NFAST * NFAST;
-    float* blk = reinterpret_cast<float*>(T + NFAST * OSW);
-    double* red = reinterpret_cast<double*>(blk + NFAST * NFAST);
-    const float* osD = reinterpret_cast<const float*>(osD2);
     float* zf = reinterpret_cast<float*>(z);
     const int tid = threadIdx.x;
-
-    for (int e = tid; e < WS; e += NT) {
-        twWs[e] = a.twWs[e];
-        tau[e] = a.tau[e];
+    const float2* twWs;
+    const float2* tau;
+    const float2* twN;
+    const float* osD;
+    float2* Yb;
+    float2* T;
+    float* blk;
+    double* red;
+    if constexpr (M::LEAN) {
+        twWs = a.twWs;
+        tau = a.tau;
+        twN = a.tw2Ws;
+        osD = reinterpret_cast<const float*>(a.osD);
+        Yb = F;  // the spectrum buffer is idle once the pair plane is formed
+        T = Yb + NFAST * NFAST;
+        blk = reinterpret_cast<float*>(T + NFAST * OSW);
+        red = reinterpret_cast<double*>(z + M::ZS);
+    } else {
+        float2* sTwWs = z + M::ZS;
+        float2* sTau = sTwWs + WS;
+        float2* sTwN = sTau + WS;
+        float2* osD2 = sTwN + N;  // 16-byte aligned: every region before it has an even float2 count
+        Yb = osD2 + M::OSD;
+        T = Yb + NFAST * NFAST;
+        blk = reinterpret_cast<float*>(T + NFAST * OSW);
+        red = reinterpret_cast<double*>(blk + NFAST * NFAST);
+        for (int e = tid; e < WS; e += NT) {
+            sTwWs[e] = a.twWs[e];
+            sTau[e] = a.tau[e];
+        }
+        for (int e = tid; e < N; e += NT) sTwN[e] = a.tw2Ws[e];
+        for (int e = tid; e < M::OSD; e += NT) osD2[e] = a.osD[e];
+        __syncthreads();
+        twWs = sTwWs;
+        tau = sTau;
+        twN = sTwN;
+        osD = reinterpret_cast<const float*>(osD2);
     }
-    for (int e = tid; e < N; e += NT) twN[e] = a.tw2Ws[e];
-    for (int e = tid; e < M::OSD; e += NT) osD2[e] = a.osD[e];
-    __syncthreads();
 
     const bool isFloat = a.sampleType == SB_CFLOAT32;
     const float thr = isFloat ? 1.0e-15f : 1.0e-6f;
@@ -386,7 +415,7 @@ static int occupancy_amps()
     return nb;
 }
 
-bool amps_supported(int Ws) { return Ws == 16 || Ws == 24 || Ws == 32 || Ws == 48; }
+bool amps_supported(int Ws) { return Ws == 16 || Ws == 24 || Ws == 32 || Ws == 48 || Ws == 64; }
 
 int amps_blocks_per_sm(int Ws)
 {
@@ -395,6 +424,7 @@ int amps_blocks_per_sm(int Ws)
     case 24: return occupancy_amps<24, 192>();
     case 32: return occupancy_amps<32, 256>();
     case 48: return occupancy_amps<48, 192>();
+    case 64: return occupancy_amps<64, 256>();
     default: return 0;
     }
 }
@@ -406,6 +436,7 @@ cudaError_t launch_strack_amps(int Ws, const AmpArgs& a, int nCta, cudaStream_t 
     case 24: return launch_amps<24, 192>(a, nCta, st);
     case 32: return launch_amps<32, 256>(a, nCta, st);
     case 48: return launch_amps<48, 192>(a, nCta, st);
+    case 64: return launch_amps<64, 256>(a, nCta, st);
     default: return cudaErrorInvalidValue;
     }
 }

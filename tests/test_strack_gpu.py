@@ -78,6 +78,15 @@ def test_window_64(ctx, pair_1k):
     _check(ctx, p, a, b)
 
 
+def test_amplitude_only_window_64(ctx, pair_1k):
+    """Amplitude tries at window 64: the small try in the lean shared-memory
+    layout (tables read from global memory), the large one (128) staged."""
+    a, b = pair_1k
+    p = _p(noComplex=1, wR=64, wA=64, wRa=64, wAa=64, deltaR=24, deltaA=24, nR=40, nA=20, rStart=64, aStart=64)
+    g, o, st = _check(ctx, p, a, b)
+    assert (o["type"] == abi.SB_AMPMATCH).sum() > 300
+
+
 def test_low_coherence_exercises_fallbacks(ctx):
     s1, s2 = synth.make_pair(512, 512, 21, dr=lambda y, x: 1.3 + 0 * x, da=lambda y, x: -0.6 + 0 * y,
                              coherence=0.25)
@@ -193,7 +202,9 @@ def test_interferogram_phase_correction(ctx):
 @pytest.mark.parametrize("kw", [
     dict(),                                                      # complex matches, 2-D fit on the 2x grid
     dict(noComplex=1),                                           # amplitude: shared-memory kernel (Ws 32)
-    dict(noComplex=1, wRa=48, wAa=48, rStart=56, aStart=56),     # amplitude: staged kernel (Ws 48)
+    dict(noComplex=1, wRa=48, wAa=48, rStart=56, aStart=56),     # amplitude: shared-memory kernel (Ws 48)
+    dict(noComplex=1, wR=64, wA=64, wRa=64, wAa=64, deltaR=24, deltaA=24, nR=36, nA=16, rStart=64,
+         aStart=64),                                             # amplitude: lean shared-memory kernel (Ws 64)
     dict(wR=64, wA=64, wRa=64, wAa=64, deltaR=24, deltaA=24, nR=36, nA=16, rStart=64, aStart=64),
 ])
 def test_gauss_fit_mode(ctx, pair_1k, kw):
