@@ -861,6 +861,29 @@ def run_other(args):
                           "cpu_baseline": {"value": cpu, "unit": "patches/s", "cores": len(blocks), "kind": "port",
                                            "sample": "whole grid, f32 CPU restatement"},
                           "clocks": clk})
+    elif args.workload == "amp64":
+        # amplitude-only tracking at window 64 (small try 64, large try 128):
+        # 2048 x 4096 pair, coherence 0.6, step 32
+        s1, s2 = synth.make_pair(2048, 4096, 11, dr=lambda y, x: 1.5 + torch.sin(2 * np.pi * x / 900),
+                                 da=lambda y, x: 0.5 * torch.cos(2 * np.pi * y / 700), coherence=0.6, device="cuda")
+        a, b = synth.to_numpy(s1), synth.to_numpy(s2)
+        Wa = 64
+        grid = dict(rStart=2 * Wa, aStart=2 * Wa, deltaR=32, deltaA=32, nR=(4096 - 4 * Wa) // 32 + 1,
+                    nA=(2048 - 4 * Wa) // 32 + 1, wR=Wa, wA=Wa, wRa=Wa, wAa=Wa, noComplex=1)
+        p = abi.TrackParams(**grid)
+        clocks.start()
+        ms = _time_calls(ctx, lambda: ctx.strack(p, s1, s2), args.steps, args.warmup)
+        clk = clocks.stop()
+        st = ctx.stage_timing()
+        res = ctx.strack(p, a, b)
+        n = grid["nR"] * grid["nA"]
+        step = max(1, grid["nA"] // cores)
+        blocks = [(i0, 1, 0, grid["nR"]) for i0 in range(0, grid["nA"], step)][:cores]
+        r64, _ = _oracle_bands("strack", a, b, grid, blocks, 4 * Wa + 48, "f64")
+        lines.append({"workload": "amplitude-only strack 2048x4096 w64 step 32 (small try 64, large try 128)",
+                      "patches": n, "value": n / (np.median(ms) * 1e-3), "unit": "patches/s",
+                      "latency_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99))},
+                      "stages": st, "accuracy": _accuracy(r64, blocks, res), "clocks": clk})
     elif args.workload in ("cfg3", "cfg3small"):
         na, nr = (8000, 16000) if args.workload == "cfg3" else (2000, 4000)
         s1, s2 = synth.shear_pair(device="cuda", na=na, nr=nr, seed=3)
@@ -941,16 +964,18 @@ def main():
     ap.add_argument("--max-batch", type=int, default=1,
                     help="job server: queued strack jobs of one window that may share one sb_strack_batch call "
                          "(cfg4/cfg5; 1: every job its own call -- batches of varying size grow the contexts' "
-                         "buffers while timed, and a buffer's reallocation waits for the whole device)")
+                         "buffers while timed)")
     ap.add_argument("--batch", type=int, default=32768, help="patches per batch in --workload dftgemm")
-    ap.add_argument("--workload", default="large", choices=["large", "small", "cfg1", "cfg3", "cfg3small", "cfg4", "cfg5", "cull", "dftgemm"],
+    ap.add_argument("--workload", default="large",
+                    choices=["large", "small", "cfg1", "cfg3", "cfg3small", "cfg4", "cfg5", "cull", "dftgemm", "amp64"],
                     help="small: 2400x4800 profiling case of the same generator; cfg1 / cfg3 / cull: the "
                          "other configurations (one JSON line each, not the bench line); cfg3small: the cfg3 "
-                         "geometry on a 2000x4000 pair (profiling case)")
+                         "geometry on a 2000x4000 pair (profiling case); amp64: amplitude-only tracking at "
+                         "window 64")
     args = ap.parse_args()
     if args.workload == "small":
         use_small_workload()
-    if args.workload in ("cfg1", "cfg3", "cfg3small", "cfg4", "cfg5", "cull", "dftgemm"):
+    if args.workload in ("cfg1", "cfg3", "cfg3small", "cfg4", "cfg5", "cull", "dftgemm", "amp64"):
         return run_other(args)
     if args.impl == "reference":
         return run_reference(args)
