@@ -542,14 +542,17 @@ __device__ __forceinline__ void staged_rows(float2* gout, Src src, float2* tile,
 }
 
 // Column pass of a staged N x N transform: column c becomes DFT_N(src(., c)),
-// handed element by element to dst(k, c, value).
-template <int N, int DIR, int NT, bool THREE, typename Src, typename Dst>
-__device__ __forceinline__ void staged_cols(Src src, Dst dst, float2* tile, float2* tileB,
-                                            const float2* __restrict__ tw)
+// handed element by element to dst(k, c, value).  keep(c0) (uniform across
+// the block) skips the tile of columns c0 .. c0+G-1 when false: a pass whose
+// consumer reads only some columns transforms only the tiles holding them.
+template <int N, int DIR, int NT, bool THREE, typename Src, typename Dst, typename Keep>
+__device__ __forceinline__ void staged_cols_if(Src src, Dst dst, Keep keep, float2* tile, float2* tileB,
+                                               const float2* __restrict__ tw)
 {
     constexpr int G = StagedTile<N, THREE>::G;
     const int tid = threadIdx.x;
     for (int c0 = 0; c0 < N; c0 += G) {
+        if (!keep(c0)) continue;
 #pragma unroll 4
         for (int e = tid; e < N * G; e += NT) {
             const int k = e / G, l = e % G;
@@ -564,6 +567,13 @@ __device__ __forceinline__ void staged_cols(Src src, Dst dst, float2* tile, floa
         }
         __syncthreads();
     }
+}
+
+template <int N, int DIR, int NT, bool THREE, typename Src, typename Dst>
+__device__ __forceinline__ void staged_cols(Src src, Dst dst, float2* tile, float2* tileB,
+                                            const float2* __restrict__ tw)
+{
+    staged_cols_if<N, DIR, NT, THREE>(src, dst, [](int) { return true; }, tile, tileB, tw);
 }
 
 // 2-D transform of an N x N row-major array anywhere in memory (row stride N;

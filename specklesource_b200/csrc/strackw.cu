@@ -235,6 +235,12 @@ __global__ void __launch_bounds__(SwCfg<W>::NT, SwCfg<W>::CTAS) strackw_kernel(S
         // F tau) serve the four parities, and each column pass reads its R with
         // the roll and tau_e1 folded into the gather and writes |c|^2 * scale
         // straight into the intensity plane.
+        // intensity columns of image 2 that detectPatch reads: the chip
+        // [eR OS, eR OS + wR2) widened by the range box sum (navgR) and one
+        // column of slack, as parity-plane columns
+        constexpr int GW = sbfft::StagedTile<W, true>::G;
+        const int cLo = max(0, eR * OS - a.navgR - 1) / 2;
+        const int cHi = min(N - 1, eR * OS + wR2 + a.navgR) / 2;
 #pragma unroll 1
         for (int q = 0; q < 2; ++q) {
             float2* F = q == 0 ? F1 : F2;
@@ -257,7 +263,13 @@ __global__ void __launch_bounds__(SwCfg<W>::NT, SwCfg<W>::CTAS) strackw_kernel(S
                 auto dst = [I, sc, e1, e2](int k, int c, float2 v) {
                     I[(size_t)(2 * k + e1) * N + 2 * c + e2] = (v.x * v.x + v.y * v.y) * sc;
                 };
-                sbfft::staged_cols<W, 1, NT, true>(src, dst, tile, tileB, twW);
+                // the chip (image 2) reads only the intensity columns of the
+                // chip and its box-sum margin: column c of a parity plane
+                // lands in intensity columns 2c and 2c + 1, so tiles of c
+                // outside [cLo, cHi] are skipped (image 1: every column)
+                sbfft::staged_cols_if<W, 1, NT, true>(
+                    src, dst, [q, cLo, cHi](int c0) { return q == 0 || (c0 + GW - 1 >= cLo && c0 <= cHi); }, tile,
+                    tileB, twW);
             }
         }
         // ------------------------------------------------ detectPatch
@@ -451,11 +463,14 @@ __global__ void __launch_bounds__(SwCfg<W>::NT, SwCfg<W>::CTAS) strackw_kernel(S
             sbfft::staged_rows<N, 1, NT, true>(Zi, srcInv, tile, tileB, twN);
             const int nLo = LA - OS * eA, nHi = N - OS * eA;  // lag rows/cols used: [0, nLo) and [nHi, N)
             auto need = [nLo, nHi](int x) { return x < nLo || x >= nHi; };
-            sbfft::staged_cols<N, 1, NT, true>([Zi](int k, int c) { return Zi[(size_t)k * N + c]; },
-                                               [Zi, need](int k, int c, float2 v) {
-                                                   if (need(k) && need(c)) Zi[(size_t)k * N + c] = v;
-                                               },
-                                               tile, tileB, twN);
+            // tiles of columns that hold no lag are not transformed
+            constexpr int GN = sbfft::StagedTile<N, true>::G;
+            sbfft::staged_cols_if<N, 1, NT, true>([Zi](int k, int c) { return Zi[(size_t)k * N + c]; },
+                                                  [Zi, need](int k, int c, float2 v) {
+                                                      if (need(k) && need(c)) Zi[(size_t)k * N + c] = v;
+                                                  },
+                                                  [nLo, nHi](int c0) { return c0 < nLo || c0 + GN - 1 >= nHi; },
+                                                  tile, tileB, twN);
         }
         // ------------------------------------------------ getPeakCorr
         const double wR2p = W - 2 * eR, wA2p = W - 2 * eA;
