@@ -280,8 +280,15 @@ __global__ void __launch_bounds__(SwCfg<W>::NT, SwCfg<W>::CTAS) strackw_kernel(S
         const int kmax = eR * OS + wA2 + a.navgA - 1;
         const int lmax = eR * OS + wR2 + a.navgR - 1;
         if (smooth) {
+            // the chip's azimuth sums read H2 only on rows clamp(i + m, 0,
+            // kmax) of the chip rows i and on the chip columns: H2 is formed
+            // there (one row and column of slack), H1 everywhere
+            const int hr0 = max(0, min(kmax, eA * OS - a.navgA) - 1);
+            const int hr1 = min(N - 1, min(kmax, eA * OS + wA2 - 1 + a.navgA) + 1);
+            const int hc0 = max(0, eR * OS - 1), hc1 = min(N - 1, eR * OS + wR2);
             for (int e = tid; e < N * N; e += NT) {
                 const int i = e / N, j = e % N;
+                const bool need2 = i >= hr0 && i <= hr1 && j >= hc0 && j <= hc1;
                 float h1 = 0.f, h2 = 0.f;
                 for (int nn = -a.navgR; nn <= a.navgR; nn++) {
                     int l = j + nn;
@@ -289,10 +296,10 @@ __global__ void __launch_bounds__(SwCfg<W>::NT, SwCfg<W>::CTAS) strackw_kernel(S
                     const int l1 = l < N - 1 ? l : N - 1;
                     const int l2 = l < lmax ? l : lmax;
                     h1 += I1[(size_t)i * N + l1];
-                    h2 += I2[(size_t)i * N + l2];
+                    if (need2) h2 += I2[(size_t)i * N + l2];
                 }
                 H1[e] = h1;
-                H2[e] = h2;
+                if (need2) H2[e] = h2;
             }
             __syncthreads();
         }
