@@ -2,8 +2,8 @@
 //
 //  cullSTData (cullSTData.c:13-125): the median test runs in place in raster
 //    order, so a cull changes the neighbourhoods of later points.  The GPU
-//    first solves that recurrence as a parallel fixpoint (cull_fix_kernel,
-//    exact when it converges); otherwise it keeps the order with a row
+//    first solves that recurrence as a parallel fixpoint (cull_fix_kernel on
+//    revisit lists, exact when it converges); otherwise it keeps the order with a row
 //    wavefront: one warp per grid row
 //    (rows claimed in increasing order from a counter, so the row a warp waits
 //    on is always held by a running warp), each warp walks its row left to
@@ -250,19 +250,23 @@ __global__ void cull_median_kernel(CullArgs a, long long spinLimit)
 // has exactly one solution, the sequential result.  Jacobi iteration
 // C_{t+1} = decide(., C_t) from C_0 = 0 reaches it, and a step that changes
 // nothing proves it was reached (a fixpoint of the recurrence is its solution).
-// A point is recomputed only when a predecessor in its box changed in the
-// previous step.  offR/offA are not modified until the fixpoint is applied;
+// Step t decides only the points on its revisit list (every point at t = 0;
+// after that the later box neighbours of the points that flipped in step
+// t - 1): any other point has no predecessor that changed, so its decision
+// is already C_t's.  The decisions of a step are read from C_t and the flips
+// applied afterwards (cull_fix_apply_kernel), so every step is exactly a
+// Jacobi step.  offR/offA are not modified until the fixpoint is applied;
 // one warp per point, medians as in the wavefront kernel.
 struct FixArgs {
     const float* offR;
     const float* offA;
-    const uint8_t* cin;
-    uint8_t* cout;
-    const uint8_t* chgIn;  // null: first step, every point computed
-    uint8_t* chgOut;
+    const uint8_t* c;        // C_t
+    const int* list;         // revisit list; null: every point (step 0)
+    const unsigned* count;   // its length (ignored when list is null)
+    int* flipped;            // points whose decision flips in this step
+    unsigned* nFlipped;
     int nR, nA, bR, bA;
     StRule rule;
-    unsigned int* nChanged;
 };
 
 template <int NV>
@@ -270,29 +274,15 @@ __global__ void cull_fix_kernel(FixArgs a)
 {
     const int lane = threadIdx.x & 31;
     const int hA = a.bA / 2, hR = a.bR / 2;
-    const long long n = (long long)a.nR * a.nA;
+    const long long n = a.list ? (long long)*a.count : (long long)a.nR * a.nA;
     const long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-    unsigned int changedHere = 0;
-    for (long long p = w0; p < n; p += nw) {
+    for (long long t = w0; t < n; t += nw) {
+        const long long p = a.list ? (long long)a.list[t] : t;
         const int i = (int)(p / a.nR), j = (int)(p % a.nR);
         const int i1 = i - hA > 0 ? i - hA : 0, i2 = i + hA < a.nA - 1 ? i + hA : a.nA - 1;
         const int j1 = j - hR > 0 ? j - hR : 0, j2 = j + hR < a.nR - 1 ? j + hR : a.nR - 1;
         const int cols = j2 - j1 + 1, cnt = (i2 - i1 + 1) * cols;
-        if (a.chgIn) {
-            bool any = false;
-            for (int e = lane; e < cnt; e += 32) {
-                const long long q = (long long)(i1 + e / cols) * a.nR + (j1 + e % cols);
-                any |= q < p && a.chgIn[q];
-            }
-            if (!__any_sync(0xffffffffu, any)) {
-                if (lane == 0) {
-                    a.cout[p] = a.cin[p];
-                    a.chgOut[p] = 0;
-                }
-                continue;
-            }
-        }
         uint32_t kr[NV], ka[NV];
         uint32_t vm = 0;
         bool notSlow = false;
@@ -303,7 +293,7 @@ __global__ void cull_fix_kernel(FixArgs a)
             if (e < cnt) {
                 const long long q = (long long)(i1 + e / cols) * a.nR + (j1 + e % cols);
                 const float r = a.offR[q], az = a.offA[q];
-                if (valid_pt(r, az) && !(q < p && a.cin[q])) {
+                if (valid_pt(r, az) && !(q < p && a.c[q])) {
                     vm |= 1u << v;
                     kr[v] = fkey(r);
                     ka[v] = fkey(az);
@@ -316,15 +306,48 @@ __global__ void cull_fix_kernel(FixArgs a)
         for (int v = 0; v < NV; ++v) ngood += (vm >> v) & 1u;
         ngood = __reduce_add_sync(0xffffffffu, ngood);
         const bool cull = st_decide<NV>(a.rule, kr, ka, vm, ngood, notSlow, a.offR[p], a.offA[p]);
-        if (lane == 0) {
-            const uint8_t c = cull ? 1 : 0;
-            a.cout[p] = c;
-            const uint8_t ch = c != a.cin[p];
-            a.chgOut[p] = ch;
-            changedHere += ch;
+        if (lane == 0 && (cull ? 1 : 0) != a.c[p]) a.flipped[atomicAdd(a.nFlipped, 1u)] = (int)p;
+    }
+}
+
+// Applies a step's flips to C and lists the points to decide next: the later
+// points (raster order) whose box holds a flipped point, each once per step
+// (mark[] holds the step that listed it).  One warp per flipped point: the
+// lanes take its later box neighbours 32 at a time and reserve their list
+// slots with one atomic per warp.
+__global__ void cull_fix_apply_kernel(uint8_t* c, const int* flipped, const unsigned* nFlipped, int* next,
+                                      unsigned* nNext, int* mark, int stamp, int nR, int nA, int bR, int bA)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned nf = *nFlipped;
+    const int hA = bA / 2, hR = bR / 2;
+    const unsigned w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned nw = (gridDim.x * blockDim.x) >> 5;
+    for (unsigned k = w0; k < nf; k += nw) {
+        const int q = flipped[k];
+        if (lane == 0) c[q] ^= 1;
+        const int i = q / nR, j = q % nR;
+        const int i2 = i + hA < nA - 1 ? i + hA : nA - 1;
+        const int j1 = j - hR > 0 ? j - hR : 0, j2 = j + hR < nR - 1 ? j + hR : nR - 1;
+        const int cols = j2 - j1 + 1;
+        const int sameRow = j2 - j;                 // (i, j+1 .. j2)
+        const int total = sameRow + (i2 - i) * cols;  // then rows i+1 .. i2, columns j1 .. j2
+        for (int b = 0; b < total; b += 32) {
+            const int e = b + lane;
+            int pp = -1;
+            if (e < total) {
+                const int y = e < sameRow ? i : i + 1 + (e - sameRow) / cols;
+                const int x = e < sameRow ? j + 1 + e : j1 + (e - sameRow) % cols;
+                pp = y * nR + x;
+                if (atomicExch(mark + pp, stamp) == stamp) pp = -1;  // listed already in this step
+            }
+            const unsigned fresh = __ballot_sync(0xffffffffu, pp >= 0);
+            unsigned base = 0;
+            if (lane == 0 && fresh) base = atomicAdd(nNext, (unsigned)__popc(fresh));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (pp >= 0) next[base + __popc(fresh & ((1u << lane) - 1u))] = pp;
         }
     }
-    if (lane == 0 && changedHere) atomicAdd(a.nChanged, changedHere);
 }
 
 // Writes the culls of the converged pass; counts them.
@@ -867,28 +890,36 @@ int run_st_fixpoint(sb_context* c, const CullJob& p, const CullDev* v, int nv, i
     if (nv > 4) return SB_ERR_UNSUPPORTED;
     const long long n = (long long)p.nR * p.nA;
     cudaError_t e;
-    uint8_t* fl = (uint8_t*)sb_ctx_buf(c, "c_fix", (size_t)n * 4, &e);
-    if (!fl) return sb_ctx_fail(c, SB_ERR_NOMEM, "device allocation failed");
-    uint8_t* C[2] = {fl, fl + n};
-    uint8_t* G[2] = {fl + 2 * n, fl + 3 * n};
-    unsigned int* nChanged = (unsigned int*)(ctl + 2);
+    // C (bytes), then int arrays: two revisit lists, the flips, the marks
+    uint8_t* C = (uint8_t*)sb_ctx_buf(c, "c_fix", (size_t)n + 16 * sizeof(int) + (size_t)n * 4 * sizeof(int), &e);
+    if (!C) return sb_ctx_fail(c, SB_ERR_NOMEM, "device allocation failed");
+    int* ibase = (int*)(((uintptr_t)(C + n) + 15) & ~(uintptr_t)15);
+    int* R[2] = {ibase, ibase + n};
+    int* flipped = ibase + 2 * n;
+    int* mark = ibase + 3 * n;
+    unsigned* cnt = (unsigned*)sb_ctx_buf(c, "c_fixcnt", 4 * sizeof(unsigned), &e);  // |R0|, |R1|, flips
+    if (!cnt) return sb_ctx_fail(c, SB_ERR_NOMEM, "device allocation failed");
     cudaStream_t s = c->stream;
-    CKC(cudaMemsetAsync(C[0], 0, (size_t)n, s), "memset");
+    CKC(cudaMemsetAsync(C, 0, (size_t)n, s), "memset");
+    CKC(cudaMemsetAsync(mark, 0, (size_t)n * sizeof(int), s), "memset");
     FixArgs f;
     f.offR = v->offR; f.offA = v->offA;
+    f.c = C;
+    f.flipped = flipped;
+    f.nFlipped = cnt + 2;
     f.nR = p.nR; f.nA = p.nA; f.bR = p.bR; f.bA = p.bA;
     f.rule = p.rule;
-    f.nChanged = nChanged;
     const int threads = 256;
     long long blocks = (n * 32 + threads - 1) / threads;
     if (blocks > (long long)c->numSM * 64) blocks = (long long)c->numSM * 64;
-    int cur = 0;
+    const int ablocks = c->numSM * 16;
     for (int step = 0; step < kMaxFixSteps; ++step) {
-        f.cin = C[cur];
-        f.cout = C[cur ^ 1];
-        f.chgIn = step == 0 ? nullptr : G[cur];
-        f.chgOut = G[cur ^ 1];
-        CKC(cudaMemsetAsync(nChanged, 0, sizeof(unsigned int), s), "memset");
+        const int in = step & 1;
+        f.list = step == 0 ? nullptr : R[in];
+        f.count = cnt + in;
+        // the flips and the next list start empty
+        CKC(cudaMemsetAsync(cnt + 2, 0, sizeof(unsigned), s), "memset");
+        CKC(cudaMemsetAsync(cnt + (in ^ 1), 0, sizeof(unsigned), s), "memset");
         switch (nv) {
         case 1: cull_fix_kernel<1><<<(int)blocks, threads, 0, s>>>(f); break;
         case 2: cull_fix_kernel<2><<<(int)blocks, threads, 0, s>>>(f); break;
@@ -896,16 +927,18 @@ int run_st_fixpoint(sb_context* c, const CullJob& p, const CullDev* v, int nv, i
         default: cull_fix_kernel<4><<<(int)blocks, threads, 0, s>>>(f); break;
         }
         CKC(cudaGetLastError(), "cull_fix");
-        c->launches++;
-        unsigned int changed = 0;
-        CKC(cudaMemcpyAsync(&changed, nChanged, sizeof(changed), cudaMemcpyDeviceToHost, s), "d2h");
+        cull_fix_apply_kernel<<<ablocks, 256, 0, s>>>(C, flipped, cnt + 2, R[in ^ 1], cnt + (in ^ 1), mark, step + 1,
+                                                      p.nR, p.nA, p.bR, p.bA);  // one warp per flip
+        CKC(cudaGetLastError(), "cull_fix_apply");
+        c->launches += 2;
+        unsigned changed = 0;
+        CKC(cudaMemcpyAsync(&changed, cnt + 2, sizeof(changed), cudaMemcpyDeviceToHost, s), "d2h");
         CKC(cudaStreamSynchronize(s), "cull_fix");
-        cur ^= 1;
         if (changed == 0) {
             unsigned long long* nCulled = (unsigned long long*)(ctl + 4);
             long long ab = (n + 255) / 256;
             if (ab > (long long)c->numSM * 16) ab = (long long)c->numSM * 16;
-            cull_apply_kernel<<<(int)ab, 256, 0, s>>>(v->offR, v->offA, C[cur], n, nCulled);
+            cull_apply_kernel<<<(int)ab, 256, 0, s>>>(v->offR, v->offA, C, n, nCulled);
             CKC(cudaGetLastError(), "cull_apply");
             c->launches++;
             unsigned long long culled = 0;
